@@ -1,0 +1,200 @@
+/*
+ * rtspatial_b200 — C ABI of the B200-native spatial index.
+ *
+ * Drop-in boundary for rtspatial::SpatialIndex<float, 2>
+ * (include/rtspatial/spatial_index.cuh:62-931 in the RTSpatial project): the
+ * same operations (Init/Clear/Insert/Delete/Update/Query), the same input
+ * layouts (Envelope<Point<float,2>> = 4 floats min.x, min.y, max.x, max.y;
+ * Point<float,2> = 2 floats), the same implicit insertion-order ids and the
+ * same result contract: one (geom_id, query_id) pair per match, handed to a
+ * counting or collecting handler.  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Array arguments are device pointers, or pinned host pointers the device
+ *    can address (the reference's tests pass pinned host vectors,
+ *    test/test_point_queries.h:67-84).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ *    asynchronous with respect to the host unless noted.
+ *  - Every call returns RTS_OK or an error code; rts_last_error() gives a
+ *    per-thread message.  Nothing aborts the process (the reference aborts or
+ *    throws, spatial_index.cuh:387-389).
+ *  - Coordinates must be finite.  The contains predicates are exact for any
+ *    finite input; range-intersects is exact for finite inputs.
+ */
+#ifndef RTSPATIAL_B200_H
+#define RTSPATIAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define RTS_OK 0
+#define RTS_ERR_INVALID_ARGUMENT 1
+#define RTS_ERR_CUDA 2
+#define RTS_ERR_OUT_OF_MEMORY 3
+#define RTS_ERR_QUEUE_FULL 4   /* a collecting queue received more pairs than its capacity */
+#define RTS_ERR_CAPACITY 5     /* a size exceeds a documented maximum */
+#define RTS_ERR_UNSUPPORTED 6
+
+/* ---- predicates: values of rtspatial::Predicate (geom/predicates.h:7-10) - */
+#define RTS_PREDICATE_INTERSECTS 0
+#define RTS_PREDICATE_CONTAINS 1
+
+/* ---- handlers ------------------------------------------------------------
+ * The reference selects a device handler at shader compile time
+ * (CMakeLists.txt:73-104 force-includes default_handlers/*.h).  Here the
+ * handler is a run-time argument with the same two shipped behaviours:
+ *  RTS_HANDLER_COUNT   arg = unsigned long long* in device memory; each pair
+ *                      adds 1 (default_handlers/counting_handlers.h:7-25).
+ *  RTS_HANDLER_COLLECT arg = rts_queue* in device memory; each pair is
+ *                      appended (default_handlers/collecting_handlers.h:9-31,
+ *                      utils/queue.h:22-27).  Pairs beyond `capacity` are not
+ *                      written but still counted in *size, so after the query
+ *                      *size > capacity signals overflow and gives the size
+ *                      needed. */
+#define RTS_HANDLER_COUNT 0
+#define RTS_HANDLER_COLLECT 1
+
+/* thrust::pair<uint32_t, uint32_t> as the collecting handler writes it. */
+typedef struct rts_pair {
+  uint32_t geom_id;
+  uint32_t query_id;
+} rts_pair;
+
+/* Device-side queue with the member layout of
+ * rtspatial::dev::Queue<thrust::pair<uint32_t,uint32_t>> (utils/queue.h:60-62:
+ * ArrayView<T>{T* data; size_t size;} followed by uint32_t* last_pos). */
+typedef struct rts_queue {
+  rts_pair* data;
+  uint64_t capacity;
+  uint32_t* size;
+} rts_queue;
+
+/* thrust::pair<size_t, Envelope<Point<float,2>>> as Update takes it
+ * (spatial_index.cuh:280-281): 8-byte id, then the envelope. */
+typedef struct rts_update_entry {
+  uint64_t id;
+  float min_x, min_y, max_x, max_y;
+} rts_update_entry;
+
+/* ---- configuration ---------------------------------------------------------
+ * First block: the fields of rtspatial::Config (spatial_index.cuh:22-37),
+ * accepted for source compatibility.  ptx_root has no counterpart (there are
+ * no PTX modules to load); the OptiX build flags and the intersects cost-model
+ * fields do not change results and are ignored.
+ * Second block: this library's own structure and traversal knobs. */
+typedef struct rts_config {
+  uint64_t max_geometries;      /* capacity reserved when preallocate != 0 */
+  uint64_t max_queries;         /* accepted, no effect */
+  int32_t preallocate;
+  int32_t prefer_fast_build_geom;  /* accepted, no effect */
+  int32_t prefer_fast_build_query; /* accepted, no effect */
+  int32_t compact;                 /* accepted, no effect */
+  float geom_sample_rate;          /* accepted, no effect */
+  float query_sample_rate;         /* accepted, no effect */
+  float intersect_cost_weight;     /* accepted, no effect */
+  uint32_t max_geom_samples;       /* accepted, no effect */
+  uint32_t max_query_samples;      /* accepted, no effect */
+  uint32_t max_parallelism;        /* accepted, no effect */
+
+  int32_t node_width;     /* children per node and boxes per leaf: 4, 8, 16 or 32 */
+  int32_t traversal;      /* RTS_TRAVERSAL_* */
+  int32_t curve;          /* RTS_CURVE_*: the order leaves are packed in */
+  int32_t max_trees;      /* insert batches kept as separate sub-trees before a merge rebuild (1..16) */
+  float rebuild_fraction; /* an insert batch larger than this fraction of the index rebuilds everything */
+  int32_t sort_queries;   /* 1: visit queries in curve order (results keep the caller's query ids) */
+  float rebuild_update_fraction; /* updates since the last rebuild, as a fraction of the index,
+                                    above which Update re-sorts instead of refitting */
+  uint32_t chunk;         /* queries per device work item (0 = library default) */
+} rts_config;
+
+#define RTS_TRAVERSAL_AUTO 0
+#define RTS_TRAVERSAL_THREAD 1 /* one thread per query, loops over a node's children */
+#define RTS_TRAVERSAL_TEAM 2   /* node_width lanes per query, one child per lane */
+
+#define RTS_CURVE_MORTON 0
+#define RTS_CURVE_HILBERT 1
+
+typedef struct rts_index rts_index;
+
+/* Fills `cfg` with the reference's defaults (spatial_index.cuh:22-37) and this
+ * library's defaults for the remaining fields. */
+int rts_config_default(rts_config* cfg);
+
+/* SpatialIndex::Init (spatial_index.cuh:83-110). */
+int rts_create(const rts_config* cfg, rts_index** out);
+int rts_destroy(rts_index* index);
+
+/* SpatialIndex::Clear (spatial_index.cuh:118-129): drops every box; ids
+ * restart at 0. */
+int rts_clear(rts_index* index, void* stream);
+
+/* SpatialIndex::Insert (spatial_index.cuh:142-196): appends n envelopes
+ * (n*4 floats); they receive ids size .. size+n-1. */
+int rts_insert(rts_index* index, const float* envelopes, uint64_t n, void* stream);
+
+/* SpatialIndex::Delete (spatial_index.cuh:208-265): each listed id becomes
+ * Envelope::Invalid() (max := min) and stays indexed; ids >= size are
+ * ignored, as the reference's `idx < v_envelopes.size()` guard does. */
+int rts_delete(rts_index* index, const uint64_t* ids, uint64_t n, void* stream);
+
+/* SpatialIndex::Update (spatial_index.cuh:280-336): overwrites the listed
+ * envelopes.  Every id must be < size (the reference asserts it, :295);
+ * out-of-range entries are skipped here. */
+int rts_update(rts_index* index, const rts_update_entry* updates, uint64_t n, void* stream);
+
+/* SpatialIndex::Query(Predicate, ArrayView<point_t>, void*, cudaStream_t)
+ * (spatial_index.cuh:352-391).  Only RTS_PREDICATE_CONTAINS is defined for
+ * points (the reference aborts on any other; this returns
+ * RTS_ERR_INVALID_ARGUMENT). */
+int rts_query_points(rts_index* index, int predicate, const float* points, uint64_t n,
+                     int handler, void* arg, void* stream);
+
+/* SpatialIndex::Query(Predicate, ArrayView<envelope_t>, void*, cudaStream_t)
+ * (spatial_index.cuh:407-515): RTS_PREDICATE_CONTAINS reports boxes that
+ * contain the query box; RTS_PREDICATE_INTERSECTS reports the reference's
+ * two-pass ray-slab result set. */
+int rts_query_envelopes(rts_index* index, int predicate, const float* envelopes, uint64_t n,
+                        int handler, void* arg, void* stream);
+
+/* ---- batched queries ----------------------------------------------------
+ * Many Query calls fused into one persistent launch with a device-side work
+ * queue.  Each batch keeps its own handler/arg and its own 0-based query ids,
+ * so a batch's results equal those of the same Query call made alone. */
+#define RTS_QUERY_POINTS 0
+#define RTS_QUERY_ENVELOPES 1
+typedef struct rts_batch {
+  int32_t query_kind; /* RTS_QUERY_POINTS or RTS_QUERY_ENVELOPES */
+  int32_t predicate;  /* RTS_PREDICATE_* */
+  const float* queries;
+  uint64_t n;
+  int32_t handler;
+  int32_t reserved;
+  void* arg;
+} rts_batch;
+
+/* Runs n_batches batches (host array) in one launch.  The descriptors are
+ * staged by the library; the call returns once they are enqueued. */
+int rts_query_batched(rts_index* index, const rts_batch* batches, uint32_t n_batches,
+                      void* stream);
+
+/* ---- introspection ------------------------------------------------------ */
+uint64_t rts_size(const rts_index* index);       /* number of ids handed out */
+uint32_t rts_num_trees(const rts_index* index);  /* sub-trees currently indexed */
+/* Device bytes held by the index (SpatialIndex::PrintMemoryUsage,
+ * spatial_index.cuh:893-903). */
+uint64_t rts_memory_usage(const rts_index* index);
+/* Message of the last failing call on this thread ("" if none). */
+const char* rts_last_error(void);
+/* Library version string. */
+const char* rts_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTSPATIAL_B200_H */

@@ -1,0 +1,22 @@
+"""rtspatial_b200 — B200-native spatial index with the interface of
+``rtspatial::SpatialIndex<float, 2>``.
+
+The index, its build/refit kernels and its query kernels live in the CUDA
+library ``librtspatial_b200.so`` (C-ABI in ``include/rtspatial_b200.h``);
+this package is the host-side mirror used from Python.  Importing it does not
+require a GPU; using an index does, and fails loudly if the library is
+missing.
+"""
+from ._lib import LIB_PATH, RtsError, lib  # noqa: F401
+from .spatial_index import (  # noqa: F401
+    Config,
+    Counter,
+    Handler,
+    Predicate,
+    Queue,
+    SpatialIndex,
+    sort_pairs,
+)
+
+__all__ = ["Config", "Counter", "Handler", "Predicate", "Queue", "SpatialIndex", "sort_pairs",
+           "RtsError", "lib", "LIB_PATH"]

@@ -1,0 +1,307 @@
+// Structure maintenance kernels: curve keys, radix sort, leaf packing, level
+// refit, Delete and Update.  These replace optixAccelBuild (BUILD and UPDATE
+// operations, rtspatial details/rt_engine.h:680-903) with a linear BVH:
+// leaves sorted along a Morton or Hilbert curve of the box centres, grouped W
+// at a time, and W-wide upper levels computed as hulls of consecutive
+// entries.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "rts_internal.h"
+
+namespace rts {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__host__ __device__ inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+// Order-preserving map of floats to unsigned ints (for atomicMin/Max).
+__device__ __forceinline__ uint32_t f2ord(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t o) {
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+__device__ __forceinline__ float4 hull(float4 b) {
+  return make_float4(fminf(b.x, b.z), fminf(b.y, b.w), fmaxf(b.x, b.z), fmaxf(b.y, b.w));
+}
+
+__device__ __forceinline__ float2 center(float4 b) {
+  float4 h = hull(b);
+  return make_float2(0.5f * (h.x + h.z), 0.5f * (h.y + h.w));
+}
+
+__global__ void k_center_bounds(const float4* __restrict__ boxes, const uint32_t* __restrict__ idx,
+                                uint64_t n, uint32_t* __restrict__ out) {
+  float lx = INFINITY, ly = INFINITY, hx = -INFINITY, hy = -INFINITY;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    float2 c = center(boxes[idx ? idx[i] : i]);
+    lx = fminf(lx, c.x);
+    ly = fminf(ly, c.y);
+    hx = fmaxf(hx, c.x);
+    hy = fmaxf(hy, c.y);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lx = fminf(lx, __shfl_xor_sync(kFull, lx, o));
+    ly = fminf(ly, __shfl_xor_sync(kFull, ly, o));
+    hx = fmaxf(hx, __shfl_xor_sync(kFull, hx, o));
+    hy = fmaxf(hy, __shfl_xor_sync(kFull, hy, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&out[0], f2ord(lx));
+    atomicMin(&out[1], f2ord(ly));
+    atomicMax(&out[2], f2ord(hx));
+    atomicMax(&out[3], f2ord(hy));
+  }
+}
+
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+  x &= 0xffffu;
+  x = (x | (x << 8)) & 0x00ff00ffu;
+  x = (x | (x << 4)) & 0x0f0f0f0fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  x = (x | (x << 1)) & 0x55555555u;
+  return x;
+}
+
+// Index along the order-16 Hilbert curve of cell (x, y), x, y < 2^16 (the
+// classic iterative rotate-and-reflect conversion).
+__device__ __forceinline__ uint32_t hilbert16(uint32_t x, uint32_t y) {
+  uint32_t d = 0;
+  for (uint32_t s = 1u << 15; s > 0; s >>= 1) {
+    uint32_t rx = (x & s) ? 1u : 0u;
+    uint32_t ry = (y & s) ? 1u : 0u;
+    d += s * s * ((3u * rx) ^ ry);
+    if (ry == 0) {
+      if (rx == 1) {
+        x = 0xffffu - x;
+        y = 0xffffu - y;
+      }
+      uint32_t t = x;
+      x = y;
+      y = t;
+    }
+  }
+  return d;
+}
+
+__global__ void k_curve_keys(const float4* __restrict__ boxes, const uint32_t* __restrict__ idx,
+                             uint64_t n, const uint32_t* __restrict__ bounds, int curve,
+                             uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float lx = ord2f(bounds[0]), ly = ord2f(bounds[1]);
+  const float hx = ord2f(bounds[2]), hy = ord2f(bounds[3]);
+  const float sx = (hx > lx) ? 65535.0f / (hx - lx) : 0.0f;
+  const float sy = (hy > ly) ? 65535.0f / (hy - ly) : 0.0f;
+  const uint32_t src = idx ? idx[i] : static_cast<uint32_t>(i);
+  float2 c = center(boxes[src]);
+  uint32_t qx = __float2uint_rz(fminf(fmaxf((c.x - lx) * sx, 0.0f), 65535.0f));
+  uint32_t qy = __float2uint_rz(fminf(fmaxf((c.y - ly) * sy, 0.0f), 65535.0f));
+  keys[i] = (curve == RTS_CURVE_HILBERT) ? hilbert16(qx, qy) : (spread16(qx) | (spread16(qy) << 1));
+  vals[i] = src;
+}
+
+__global__ void k_gather(const float4* __restrict__ src, const uint32_t* __restrict__ src_ids,
+                         const uint32_t* __restrict__ order, uint64_t n, uint64_t id_begin,
+                         uint64_t slot_base, float4* __restrict__ leaves,
+                         uint32_t* __restrict__ leaf_ids, uint32_t* __restrict__ pos) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t o = order[i];
+  uint32_t id = src_ids ? src_ids[o] : static_cast<uint32_t>(id_begin + o);
+  uint64_t slot = slot_base + i;
+  leaves[slot] = src[o];
+  leaf_ids[slot] = id;
+  pos[id] = static_cast<uint32_t>(slot);
+}
+
+__global__ void k_fill_pad(float4* __restrict__ leaves, uint32_t* __restrict__ ids, uint64_t from,
+                           uint64_t to) {
+  uint64_t i = from + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= to) return;
+  leaves[i] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+  if (ids) ids[i] = 0xffffffffu;
+}
+
+// out[j] = hull of in[j*G .. j*G+G) for j < n_out_pad; entries past n_in are
+// empty.  One lane per input entry, shuffles reduce each aligned group.
+__global__ void k_pack(const float4* __restrict__ in, uint64_t n_in, float4* __restrict__ out,
+                       uint64_t n_out_pad, int log2g) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  float4 b = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+  if (i < n_in) b = hull(in[i]);
+  for (int o = 1; o < (1 << log2g); o <<= 1) {
+    b.x = fminf(b.x, __shfl_xor_sync(kFull, b.x, o));
+    b.y = fminf(b.y, __shfl_xor_sync(kFull, b.y, o));
+    b.z = fmaxf(b.z, __shfl_xor_sync(kFull, b.z, o));
+    b.w = fmaxf(b.w, __shfl_xor_sync(kFull, b.w, o));
+  }
+  uint64_t j = i >> log2g;
+  if ((i & ((1u << log2g) - 1)) == 0 && j < n_out_pad) out[j] = b;
+}
+
+__global__ void k_slot_list(const uint64_t* __restrict__ meta, int n_trees,
+                            uint32_t* __restrict__ slots) {
+  // meta: per tree {id_begin, n, slot_base}
+  int t = blockIdx.y;
+  if (t >= n_trees) return;
+  uint64_t id_begin = meta[3 * t], n = meta[3 * t + 1], slot_base = meta[3 * t + 2];
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    slots[id_begin + i] = static_cast<uint32_t>(slot_base + i);
+}
+
+// Delete: Envelope::Invalid() (max := min) on each listed id below n_ids
+// (spatial_index.cuh:216-233); the box stays in its slot.
+__global__ void k_delete(const uint64_t* __restrict__ ids, uint64_t n, uint64_t n_ids,
+                         const uint32_t* __restrict__ pos, float4* __restrict__ leaves) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t id = ids[i];
+  if (id >= n_ids) return;
+  uint32_t slot = pos[id];
+  float4 b = leaves[slot];
+  b.z = b.x;
+  b.w = b.y;
+  leaves[slot] = b;
+}
+
+// Update: overwrite the envelope of each listed id (spatial_index.cuh:289-305).
+__global__ void k_update(const rts_update_entry* __restrict__ upd, uint64_t n, uint64_t n_ids,
+                         const uint32_t* __restrict__ pos, float4* __restrict__ leaves) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  rts_update_entry e = upd[i];
+  if (e.id >= n_ids) return;
+  leaves[pos[e.id]] = make_float4(e.min_x, e.min_y, e.max_x, e.max_y);
+}
+
+inline unsigned grid_for(uint64_t n) {
+  uint64_t g = div_up(n, kThreads);
+  return static_cast<unsigned>(g ? g : 1);
+}
+
+}  // namespace
+
+void plan_levels(uint64_t n, int W, HostTree& t) {
+  for (int i = 0; i < kMaxLevels; ++i) t.level_off[i] = t.level_cnt[i] = 0;
+  t.level_cnt[0] = static_cast<uint32_t>(n);
+  uint64_t cnt = n;
+  uint64_t off = static_cast<uint64_t>(W);  // entries 0..W-1: root box + spare
+  uint32_t L = 0;
+  do {
+    ++L;
+    cnt = div_up(cnt, W);
+    t.level_cnt[L] = static_cast<uint32_t>(cnt);
+    t.level_off[L] = static_cast<uint32_t>(off);
+    off += div_up(cnt, W) * W;
+  } while (cnt > static_cast<uint64_t>(W) && L + 1 < kMaxLevels);
+  t.top = L;
+  t.node_entries = off;
+}
+
+int launch_center_bounds(const float4* boxes, const uint32_t* idx, uint64_t n, uint32_t* bounds,
+                         cudaStream_t s) {
+  RTS_CUDA_TRY(cudaMemsetAsync(bounds, 0xff, 2 * sizeof(uint32_t), s));
+  RTS_CUDA_TRY(cudaMemsetAsync(bounds + 2, 0x00, 2 * sizeof(uint32_t), s));
+  if (n == 0) return RTS_OK;
+  unsigned g = static_cast<unsigned>(div_up(n, kThreads));
+  if (g > 148u * 8u) g = 148u * 8u;
+  k_center_bounds<<<g, kThreads, 0, s>>>(boxes, idx, n, bounds);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_curve_keys(const float4* boxes, const uint32_t* idx, uint64_t n, const uint32_t* bounds,
+                      int curve, uint32_t* keys, uint32_t* vals, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_curve_keys<<<grid_for(n), kThreads, 0, s>>>(boxes, idx, n, bounds, curve, keys, vals);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
+               uint64_t n, DevBuf& temp, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  size_t need = 0;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, kin, kout, vin, vout,
+                                                static_cast<int>(n), 0, 32, s));
+  int rc = buf_reserve(temp, need, s, false, 0);
+  if (rc) return rc;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.ptr, need, kin, kout, vin, vout,
+                                                static_cast<int>(n), 0, 32, s));
+  return RTS_OK;
+}
+
+int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
+                  uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
+                  uint32_t* pos, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_gather<<<grid_for(n), kThreads, 0, s>>>(src, src_ids, order, n, id_begin, slot_base, leaves,
+                                            leaf_ids, pos);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s) {
+  if (to <= from) return RTS_OK;
+  k_fill_pad<<<grid_for(to - from), kThreads, 0, s>>>(leaves, ids, from, to);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_t s) {
+  int log2w = 0;
+  while ((1 << log2w) < W) ++log2w;
+  float4* nodes = static_cast<float4*>(t.nodes.ptr);
+  for (uint32_t L = 1; L <= t.top; ++L) {
+    const float4* in = (L == 1) ? leaves : nodes + t.level_off[L - 1];
+    uint64_t n_in = t.level_cnt[L - 1];
+    uint64_t n_out_pad = div_up(t.level_cnt[L], W) * W;
+    uint64_t threads = n_out_pad << log2w;
+    k_pack<<<grid_for(threads), kThreads, 0, s>>>(in, n_in, nodes + t.level_off[L], n_out_pad,
+                                                  log2w);
+    RTS_CUDA_TRY(cudaGetLastError());
+  }
+  // Root box and the spare entries 1..W-1 of the first group.
+  k_pack<<<grid_for(static_cast<uint64_t>(W) << log2w), kThreads, 0, s>>>(
+      nodes + t.level_off[t.top], t.level_cnt[t.top], nodes, W, log2w);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint32_t* slots,
+                     cudaStream_t s) {
+  if (n_trees == 0) return RTS_OK;
+  uint64_t gx = div_up(max_n, kThreads);
+  if (gx > 4096) gx = 4096;
+  if (gx == 0) gx = 1;
+  dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(n_trees));
+  k_slot_list<<<grid, kThreads, 0, s>>>(meta_dev, n_trees, slots);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
+                  float4* leaves, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_delete<<<grid_for(n), kThreads, 0, s>>>(ids, n, n_ids, pos, leaves);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
+                  float4* leaves, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_update<<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, leaves);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+}  // namespace rts

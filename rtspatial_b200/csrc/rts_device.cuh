@@ -1,0 +1,295 @@
+// Device-side types and exact predicates of the rtspatial_b200 index.
+//
+// Index layout in HBM (one "tree" per insert batch until a merge rebuild):
+//   leaves[slot]    float4 {min.x, min.y, max.x, max.y}: the stored envelopes,
+//                   grouped by tree and packed along a space-filling curve
+//   leaf_ids[slot]  uint32 insertion-order id of the envelope in that slot
+//   pos[id]         slot of an id (Delete/Update write through it)
+//   nodes (per tree) float4 boxes of the upper levels; level L >= 1 entry j is
+//                   the hull of entries [j*W, j*W+W) of level L-1 (level 0 =
+//                   the tree's leaves).  nodes[0] holds the tree's root box.
+// The tree is implicit: the children of level-L entry j are entries
+// [j*W, j*W+W) of level L-1, so no child pointers are stored and a refit is
+// one coalesced pass per level.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rts {
+
+constexpr int kMaxLevels = 16;
+constexpr int kMaxTrees = 16;
+constexpr uint32_t kFull = 0xffffffffu;
+
+enum PredKind : int { kPoint = 0, kContains = 1, kIntersects = 2 };
+enum HandlerKind : int { kCount = 0, kCollect = 1 };
+
+struct TreeDesc {
+  const float4* leaves;  // first slot of this tree
+  const uint32_t* ids;   // leaf_ids of the first slot
+  const float4* nodes;   // nodes[0] = root box; level L at nodes + level_off[L]
+  uint32_t n;            // envelopes in this tree
+  uint32_t top;          // highest level (>= 1); it holds <= W entries
+  uint32_t level_off[kMaxLevels];
+  uint32_t level_cnt[kMaxLevels];
+};
+
+struct Forest {
+  TreeDesc tree[kMaxTrees];
+  uint32_t n_trees;
+  uint32_t width;
+  uint32_t pad[2];
+};
+
+// Collecting handler target: member layout of
+// rtspatial::dev::Queue<thrust::pair<uint32_t,uint32_t>> (utils/queue.h:60-62).
+struct DevPair {
+  uint32_t geom_id;
+  uint32_t query_id;
+};
+struct DevQueue {
+  DevPair* data;
+  unsigned long long capacity;
+  uint32_t* size;
+};
+
+// ---------------------------------------------------------------------------
+// Exact predicates (float32, IEEE round-to-nearest, no contraction).
+// ---------------------------------------------------------------------------
+
+// nextafterf(1.0f, FLT_MAX) (details/ray_params.h:139).
+constexpr float kT1 = 0x1.000002p+0f;
+// 1 + 2 * FLT_GAMMA(3) in float arithmetic = 1 + 6 * 2^-23
+// (details/ray_params.h:40,158).
+constexpr float kSlabK = 0x1.00000cp+0f;
+
+// RayParams<float,2>::IsHit (details/ray_params.h:137-166) with the two
+// reciprocals of the ray direction supplied by the caller (the reference
+// computes the same 1/d inside the loop).  NaN slab values leave [t0, t1]
+// unchanged, like the reference's ternaries.
+__device__ __forceinline__ bool slab_hit(float ox, float oy, float invx, float invy,
+                                         float4 b) {
+  float t0 = 0.0f, t1 = kT1;
+  float tn = __fmul_rn(__fsub_rn(b.x, ox), invx);
+  float tf = __fmul_rn(__fsub_rn(b.z, ox), invx);
+  if (tn > tf) {
+    float t = tn;
+    tn = tf;
+    tf = t;
+  }
+  tf = __fmul_rn(tf, kSlabK);
+  t0 = tn > t0 ? tn : t0;
+  t1 = tf < t1 ? tf : t1;
+  if (t0 > t1) return false;
+  tn = __fmul_rn(__fsub_rn(b.y, oy), invy);
+  tf = __fmul_rn(__fsub_rn(b.w, oy), invy);
+  if (tn > tf) {
+    float t = tn;
+    tn = tf;
+    tf = t;
+  }
+  tf = __fmul_rn(tf, kSlabK);
+  t0 = tn > t0 ? tn : t0;
+  t1 = tf < t1 ? tf : t1;
+  return !(t0 > t1);
+}
+
+// Envelope::Contains(point) (geom/envelope.cuh:29-38), closed intervals.
+__device__ __forceinline__ bool contains_point(float4 g, float2 p) {
+  return p.x >= g.x && p.x <= g.z && p.y >= g.y && p.y <= g.w;
+}
+
+// Envelope::Contains(envelope) (geom/envelope.cuh:40-53).
+__device__ __forceinline__ bool contains_box(float4 g, float4 q) {
+  return q.x >= g.x && q.z <= g.z && q.y >= g.y && q.w <= g.w;
+}
+
+// Per-query state of a range-intersects query.
+struct IsectQuery {
+  float4 q;            // the query envelope
+  float ox, oy;        // origin of its anti-diagonal ray: (max.x, min.y)
+  float invx, invy;    // 1 / (min.x - max.x), 1 / (max.y - min.y)
+  float4 nb;           // hull of q inflated by the conservative margin
+};
+
+__device__ __forceinline__ IsectQuery make_isect_query(float4 q) {
+  IsectQuery Q;
+  Q.q = q;
+  // RayParams::Compute(query, true) (details/ray_params.h:67-84).
+  Q.ox = q.z;
+  Q.oy = q.y;
+  Q.invx = __frcp_rn(__fsub_rn(q.x, q.z));
+  Q.invy = __frcp_rn(__fsub_rn(q.w, q.y));
+  Q.nb = make_float4(0.f, 0.f, 0.f, 0.f);
+  return Q;
+}
+
+// Margin for the node test of range-intersects.  If the reference's
+// predicate accepts (g, q), some t* in [t0, t1] certifies it.  Along the
+// computed direction d~ = fl(p2 - p1) every slab value carries a relative
+// error <= 3u (u = 2^-24); the far value is scaled by 1 + 12u and rounded once
+// more; t* <= 1 + 2u and d~ is within u of p2 - p1.  So the point o + t* d~
+// lies within 3u|p2 - p1| of the ray's box and within 17u*max(|min - o|,
+// |max - o|) of the target box per axis: the two hulls are apart by at most
+// 40u*M, M the largest coordinate magnitude of the pair.  Zero or subnormal
+// directions give infinite or NaN slab values, which only accept when the
+// origin lies within the slab.  The margin 2^-17*M + 2^-120 = (128u)*M + tiny
+// exceeds the bound with room for the rounding of the inflated bounds.
+// mag = per-axis magnitude bound of the tree's boxes.
+__device__ __forceinline__ void isect_set_margin(IsectQuery& Q, float2 mag) {
+  const float4 q = Q.q;
+  float mx = fmaxf(mag.x, fmaxf(fabsf(q.x), fabsf(q.z)));
+  float my = fmaxf(mag.y, fmaxf(fabsf(q.y), fabsf(q.w)));
+  float ex = __fadd_rn(__fmul_rn(mx, 0x1p-17f), 0x1p-120f);
+  float ey = __fadd_rn(__fmul_rn(my, 0x1p-17f), 0x1p-120f);
+  Q.nb.x = __fsub_rn(fminf(q.x, q.z), ex);
+  Q.nb.y = __fsub_rn(fminf(q.y, q.w), ey);
+  Q.nb.z = __fadd_rn(fmaxf(q.x, q.z), ex);
+  Q.nb.w = __fadd_rn(fmaxf(q.y, q.w), ey);
+}
+
+// Closed overlap of a (hull) box with the inflated query box.
+__device__ __forceinline__ bool overlaps(float4 e, float4 nb) {
+  return e.x <= nb.z && e.z >= nb.x && e.y <= nb.w && e.w >= nb.y;
+}
+
+// Range-intersects result set of the reference for pair (g, q):
+//   backward pass (shaders_intersects_envelope_query_2d.cu:75-129): g valid
+//     and g's main diagonal hits q;
+//   forward pass (same file :14-41): q's anti-diagonal hits g and g's main
+//     diagonal misses q.
+// i.e. hit2 = IsHit(g main diagonal, q); result = hit2 ? g.IsValid() : hit1.
+__device__ __forceinline__ bool isect_exact(float4 g, const IsectQuery& Q) {
+  float gix = __frcp_rn(__fsub_rn(g.z, g.x));
+  float giy = __frcp_rn(__fsub_rn(g.w, g.y));
+  if (slab_hit(g.x, g.y, gix, giy, Q.q)) return g.x < g.z && g.y < g.w;
+  return slab_hit(Q.ox, Q.oy, Q.invx, Q.invy, g);
+}
+
+// Leaf test: the exact predicate behind the (sound) inflated-hull prefilter.
+__device__ __forceinline__ bool isect_leaf(float4 g, const IsectQuery& Q) {
+  float4 h = make_float4(fminf(g.x, g.z), fminf(g.y, g.w), fmaxf(g.x, g.z), fmaxf(g.y, g.w));
+  if (!overlaps(h, Q.nb)) return false;
+  return isect_exact(g, Q);
+}
+
+// Magnitude bound of a tree from its root box (node boxes are hulls).
+__device__ __forceinline__ float2 root_magnitude(float4 r) {
+  return make_float2(fmaxf(fabsf(r.x), fabsf(r.z)), fmaxf(fabsf(r.y), fabsf(r.w)));
+}
+
+// ---------------------------------------------------------------------------
+// Query adaptors: one per predicate, same interface.
+// ---------------------------------------------------------------------------
+template <int PRED>
+struct QueryOps;
+
+template <>
+struct QueryOps<kPoint> {
+  using Q = float2;
+  static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
+    return reinterpret_cast<const float2*>(qs)[i];
+  }
+  static __device__ __forceinline__ void enter_tree(Q&, float4) {}
+  static __device__ __forceinline__ bool node(float4 e, const Q& p) { return contains_point(e, p); }
+  static __device__ __forceinline__ bool leaf(float4 g, const Q& p) { return contains_point(g, p); }
+};
+
+template <>
+struct QueryOps<kContains> {
+  using Q = float4;
+  static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
+    return reinterpret_cast<const float4*>(qs)[i];
+  }
+  static __device__ __forceinline__ void enter_tree(Q&, float4) {}
+  // A box containing q lies inside a node hull that then contains q too.
+  static __device__ __forceinline__ bool node(float4 e, const Q& q) { return contains_box(e, q); }
+  static __device__ __forceinline__ bool leaf(float4 g, const Q& q) { return contains_box(g, q); }
+};
+
+template <>
+struct QueryOps<kIntersects> {
+  using Q = IsectQuery;
+  static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
+    return make_isect_query(reinterpret_cast<const float4*>(qs)[i]);
+  }
+  static __device__ __forceinline__ void enter_tree(Q& q, float4 root) {
+    isect_set_margin(q, root_magnitude(root));
+  }
+  static __device__ __forceinline__ bool node(float4 e, const Q& q) { return overlaps(e, q.nb); }
+  static __device__ __forceinline__ bool leaf(float4 g, const Q& q) { return isect_leaf(g, q); }
+};
+
+// ---------------------------------------------------------------------------
+// Per-level child masks of one traversal, packed W bits per level.
+// ---------------------------------------------------------------------------
+template <int W>
+struct MaskStack {
+  static constexpr int kWords = (W == 32) ? 3 : 2;
+  static constexpr int kLevels = kWords * 64 / W;  // levels 1..kLevels storable
+  static constexpr uint64_t kMask = (W == 32) ? 0xffffffffull : ((1ull << W) - 1ull);
+  uint64_t w[kWords];
+
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int i = 0; i < kWords; ++i) w[i] = 0;
+  }
+  __device__ __forceinline__ uint32_t get(int level) const {
+    int off = (level - 1) * W;
+    int wi = off >> 6, sh = off & 63;
+    uint64_t v = 0;
+#pragma unroll
+    for (int i = 0; i < kWords; ++i) v = (i == wi) ? w[i] : v;
+    return static_cast<uint32_t>((v >> sh) & kMask);
+  }
+  __device__ __forceinline__ void set(int level, uint32_t m) {
+    int off = (level - 1) * W;
+    int wi = off >> 6, sh = off & 63;
+#pragma unroll
+    for (int i = 0; i < kWords; ++i)
+      if (i == wi) w[i] = (w[i] & ~(kMask << sh)) | (static_cast<uint64_t>(m) << sh);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Output: the two handler behaviours, warp-aggregated.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Appends, for every lane, the pairs (ids[c], qid) for each set bit c of m.
+// Must be called by all 32 lanes.  One atomicAdd per warp; the queue's
+// counter keeps counting past capacity so the caller can see the size needed.
+__device__ __forceinline__ void collect_warp(const DevQueue& qu, uint32_t m,
+                                             const uint32_t* ids, uint32_t qid) {
+  const uint32_t lane = lane_id();
+  uint32_t cnt = __popc(m);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= static_cast<uint32_t>(o)) incl += v;
+  }
+  uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  uint32_t base = 0;
+  if (lane == 31) base = atomicAdd(qu.size, total);
+  base = __shfl_sync(kFull, base, 31);
+  unsigned long long p = static_cast<unsigned long long>(base) + (incl - cnt);
+  while (m) {
+    int c = __ffs(m) - 1;
+    m &= m - 1;
+    if (p < qu.capacity) qu.data[p] = DevPair{ids[c], qid};
+    ++p;
+  }
+}
+
+// Lane-count reduction for the counting handler, one atomic per warp.
+__device__ __forceinline__ void count_flush_warp(unsigned long long* counter,
+                                                 unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  if (lane_id() == 0 && v) atomicAdd(counter, v);
+}
+
+}  // namespace rts

@@ -1,0 +1,557 @@
+// C-ABI implementation: the index manager behind rtspatial::SpatialIndex.
+//
+// State per index: the leaf slots (boxes + ids, grouped per sub-tree), the
+// id -> slot map, and one W-wide implicit tree per sub-tree.  Insert builds a
+// sub-tree for the new batch (the reference builds one GAS per batch and an
+// IAS over all of them, spatial_index.cuh:142-196); after max_trees sub-trees,
+// or for a batch larger than rebuild_fraction of the index, all boxes are
+// re-sorted into a single tree.  Delete collapses boxes in place (node boxes
+// stay conservative, no refit needed); Update overwrites boxes and refits every
+// sub-tree, or re-sorts once the updates since the last rebuild exceed
+// rebuild_update_fraction of the index.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rts_internal.h"
+
+namespace rts {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return (e == cudaErrorMemoryAllocation) ? RTS_ERR_OUT_OF_MEMORY : RTS_ERR_CUDA;
+}
+
+int buf_reserve(DevBuf& b, size_t bytes, cudaStream_t s, bool keep, size_t used) {
+  if (bytes <= b.bytes && b.ptr) return RTS_OK;
+  size_t cap = std::max(bytes, b.bytes + b.bytes / 2);
+  cap = (cap + 255) & ~static_cast<size_t>(255);
+  void* p = nullptr;
+  RTS_CUDA_TRY(cudaMallocAsync(&p, cap, s));
+  if (keep && b.ptr && used) {
+    cudaError_t e = cudaMemcpyAsync(p, b.ptr, std::min(used, b.bytes), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(p, s);
+      return cuda_fail(e, "cudaMemcpyAsync(grow)");
+    }
+  }
+  if (b.ptr) cudaFreeAsync(b.ptr, s);
+  b.ptr = p;
+  b.bytes = cap;
+  return RTS_OK;
+}
+
+void buf_free(DevBuf& b, cudaStream_t s) {
+  if (b.ptr) cudaFreeAsync(b.ptr, s);
+  b.ptr = nullptr;
+  b.bytes = 0;
+}
+
+static inline uint64_t round_up(uint64_t a, uint64_t b) { return (a + b - 1) / b * b; }
+
+// Levels storable by the traversal's mask stack at each width.
+static uint32_t max_levels_for(int W) {
+  switch (W) {
+    case 4: return MaskStack<4>::kLevels;
+    case 8: return MaskStack<8>::kLevels;
+    case 16: return MaskStack<16>::kLevels;
+    case 32: return MaskStack<32>::kLevels;
+  }
+  return 0;
+}
+
+// Pinned staging for small host->device copies that must not block the host:
+// a ring of slots, each reused only after the copy that last read it is done.
+struct Staging {
+  static constexpr int kSlots = 4;
+  void* host[kSlots] = {};
+  DevBuf dev[kSlots];
+  size_t host_bytes[kSlots] = {};
+  cudaEvent_t done[kSlots] = {};
+  int next = 0;
+
+  // Copies `bytes` from src to a device buffer; returns its device address.
+  int put(const void* src, size_t bytes, cudaStream_t s, void** dev_out) {
+    int k = next;
+    next = (next + 1) % kSlots;
+    if (done[k]) RTS_CUDA_TRY(cudaEventSynchronize(done[k]));
+    else RTS_CUDA_TRY(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+    if (host_bytes[k] < bytes) {
+      if (host[k]) cudaFreeHost(host[k]);
+      host[k] = nullptr;
+      size_t cap = std::max<size_t>(bytes, 4096);
+      RTS_CUDA_TRY(cudaMallocHost(&host[k], cap));
+      host_bytes[k] = cap;
+    }
+    int rc = buf_reserve(dev[k], bytes, s, false, 0);
+    if (rc) return rc;
+    std::memcpy(host[k], src, bytes);
+    RTS_CUDA_TRY(cudaMemcpyAsync(dev[k].ptr, host[k], bytes, cudaMemcpyHostToDevice, s));
+    RTS_CUDA_TRY(cudaEventRecord(done[k], s));
+    *dev_out = dev[k].ptr;
+    return RTS_OK;
+  }
+  void release() {
+    for (int k = 0; k < kSlots; ++k) {
+      if (done[k]) {
+        cudaEventSynchronize(done[k]);
+        cudaEventDestroy(done[k]);
+        done[k] = nullptr;
+      }
+      if (host[k]) cudaFreeHost(host[k]);
+      host[k] = nullptr;
+      host_bytes[k] = 0;
+      buf_free(dev[k], 0);
+    }
+  }
+};
+
+}  // namespace rts
+
+using namespace rts;
+
+struct rts_index {
+  rts_config cfg{};
+  int W = 8;
+  uint64_t n_ids = 0;
+  uint64_t slot_end = 0;        // slots in use (each sub-tree padded to 32)
+  uint64_t updated_since_build = 0;
+  DevBuf leaves, leaf_ids, pos;
+  std::vector<HostTree> trees;
+  // scratch of the build path
+  DevBuf keys_a, keys_b, vals_a, vals_b, sort_temp, bounds, slots_tmp;
+  // scratch of the query path
+  DevBuf work;
+  Staging staging;
+  Forest forest{};
+  bool forest_dirty = true;
+};
+
+namespace {
+
+constexpr uint64_t kSlotAlign = 32;
+
+int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
+  uint64_t need = slots + kSlotAlign;
+  int rc = buf_reserve(ix->leaves, need * sizeof(float4), s, true, ix->slot_end * sizeof(float4));
+  if (rc) return rc;
+  return buf_reserve(ix->leaf_ids, need * sizeof(uint32_t), s, true,
+                     ix->slot_end * sizeof(uint32_t));
+}
+
+int ensure_ids(rts_index* ix, uint64_t ids, cudaStream_t s) {
+  return buf_reserve(ix->pos, std::max<uint64_t>(ids, 1) * sizeof(uint32_t), s, true,
+                     ix->n_ids * sizeof(uint32_t));
+}
+
+int ensure_sort_scratch(rts_index* ix, uint64_t n, cudaStream_t s) {
+  size_t b = std::max<uint64_t>(n, 1) * sizeof(uint32_t);
+  int rc;
+  if ((rc = buf_reserve(ix->keys_a, b, s, false, 0))) return rc;
+  if ((rc = buf_reserve(ix->keys_b, b, s, false, 0))) return rc;
+  if ((rc = buf_reserve(ix->vals_a, b, s, false, 0))) return rc;
+  if ((rc = buf_reserve(ix->vals_b, b, s, false, 0))) return rc;
+  return buf_reserve(ix->bounds, 4 * sizeof(uint32_t), s, false, 0);
+}
+
+float4* leaves_of(rts_index* ix) { return static_cast<float4*>(ix->leaves.ptr); }
+uint32_t* ids_of(rts_index* ix) { return static_cast<uint32_t*>(ix->leaf_ids.ptr); }
+uint32_t* pos_of(rts_index* ix) { return static_cast<uint32_t*>(ix->pos.ptr); }
+
+// Allocates the node buffer of `t` and packs its levels from its leaves.
+int build_tree_levels(rts_index* ix, HostTree& t, cudaStream_t s) {
+  plan_levels(t.n, ix->W, t);
+  if (t.top > max_levels_for(ix->W))
+    return fail(RTS_ERR_CAPACITY, "sub-tree too deep for node width " + std::to_string(ix->W));
+  int rc = buf_reserve(t.nodes, t.node_entries * sizeof(float4), s, false, 0);
+  if (rc) return rc;
+  return launch_pack_tree(leaves_of(ix) + t.slot_base, t, ix->W, s);
+}
+
+// Sorts `n` boxes (src[idx[i]] or src[i]) along the curve, writes them and
+// their ids to slots [slot_base, slot_base + n), and records pos[].
+int sort_into_slots(rts_index* ix, const float4* src, const uint32_t* src_ids, const uint32_t* idx,
+                    uint64_t n, uint64_t id_begin, uint64_t slot_base, float4* dst_leaves,
+                    uint32_t* dst_ids, cudaStream_t s) {
+  int rc = ensure_sort_scratch(ix, n, s);
+  if (rc) return rc;
+  auto* bounds = static_cast<uint32_t*>(ix->bounds.ptr);
+  auto* ka = static_cast<uint32_t*>(ix->keys_a.ptr);
+  auto* kb = static_cast<uint32_t*>(ix->keys_b.ptr);
+  auto* va = static_cast<uint32_t*>(ix->vals_a.ptr);
+  auto* vb = static_cast<uint32_t*>(ix->vals_b.ptr);
+  if ((rc = launch_center_bounds(src, idx, n, bounds, s))) return rc;
+  if ((rc = launch_curve_keys(src, idx, n, bounds, ix->cfg.curve, ka, va, s))) return rc;
+  if ((rc = sort_pairs(ka, kb, va, vb, n, ix->sort_temp, s))) return rc;
+  if ((rc = launch_gather(src, src_ids, vb, n, id_begin, slot_base, dst_leaves, dst_ids,
+                          pos_of(ix), s)))
+    return rc;
+  return launch_fill_pad(dst_leaves, dst_ids, slot_base + n, slot_base + round_up(n, kSlotAlign), s);
+}
+
+// Re-sorts every box of the index into one tree.
+int rebuild_all(rts_index* ix, cudaStream_t s) {
+  const uint64_t N = ix->n_ids;
+  int rc;
+  if (N == 0) return RTS_OK;
+  // slots_tmp[k] = slot of the k-th id-ordered entry, tree by tree.
+  std::vector<uint64_t> meta;
+  uint64_t max_n = 0;
+  for (auto& t : ix->trees) {
+    meta.push_back(t.id_begin);
+    meta.push_back(t.n);
+    meta.push_back(t.slot_base);
+    max_n = std::max(max_n, t.n);
+  }
+  void* meta_dev = nullptr;
+  if ((rc = ix->staging.put(meta.data(), meta.size() * sizeof(uint64_t), s, &meta_dev))) return rc;
+  if ((rc = buf_reserve(ix->slots_tmp, N * sizeof(uint32_t), s, false, 0))) return rc;
+  auto* slots = static_cast<uint32_t*>(ix->slots_tmp.ptr);
+  if ((rc = launch_slot_list(static_cast<const uint64_t*>(meta_dev), static_cast<int>(ix->trees.size()),
+                             max_n, slots, s)))
+    return rc;
+  // New slot arrays; the old ones are read by the gather.
+  DevBuf new_leaves, new_ids;
+  const uint64_t slots_needed = round_up(N, kSlotAlign);
+  if ((rc = buf_reserve(new_leaves, std::max(ix->leaves.bytes, (slots_needed + kSlotAlign) * sizeof(float4)), s, false, 0)))
+    return rc;
+  if ((rc = buf_reserve(new_ids, std::max(ix->leaf_ids.bytes, (slots_needed + kSlotAlign) * sizeof(uint32_t)), s, false, 0))) {
+    buf_free(new_leaves, s);
+    return rc;
+  }
+  rc = sort_into_slots(ix, leaves_of(ix), ids_of(ix), slots, N, 0, 0,
+                       static_cast<float4*>(new_leaves.ptr), static_cast<uint32_t*>(new_ids.ptr), s);
+  if (rc) {
+    buf_free(new_leaves, s);
+    buf_free(new_ids, s);
+    return rc;
+  }
+  buf_free(ix->leaves, s);
+  buf_free(ix->leaf_ids, s);
+  ix->leaves = new_leaves;
+  ix->leaf_ids = new_ids;
+  for (auto& t : ix->trees) buf_free(t.nodes, s);
+  ix->trees.clear();
+  HostTree t;
+  t.id_begin = 0;
+  t.n = N;
+  t.slot_base = 0;
+  ix->slot_end = slots_needed;
+  if ((rc = build_tree_levels(ix, t, s))) return rc;
+  ix->trees.push_back(t);
+  ix->updated_since_build = 0;
+  ix->forest_dirty = true;
+  return RTS_OK;
+}
+
+void refresh_forest(rts_index* ix) {
+  if (!ix->forest_dirty) return;
+  Forest& F = ix->forest;
+  std::memset(&F, 0, sizeof(F));
+  F.n_trees = static_cast<uint32_t>(ix->trees.size());
+  F.width = static_cast<uint32_t>(ix->W);
+  for (size_t i = 0; i < ix->trees.size(); ++i) {
+    const HostTree& h = ix->trees[i];
+    TreeDesc& d = F.tree[i];
+    d.leaves = leaves_of(ix) + h.slot_base;
+    d.ids = ids_of(ix) + h.slot_base;
+    d.nodes = static_cast<const float4*>(h.nodes.ptr);
+    d.n = static_cast<uint32_t>(h.n);
+    d.top = h.top;
+    for (int L = 0; L < kMaxLevels; ++L) {
+      d.level_off[L] = h.level_off[L];
+      d.level_cnt[L] = h.level_cnt[L];
+    }
+  }
+  ix->forest_dirty = false;
+}
+
+LaunchPlan plan_for(const rts_index* ix, int pred) {
+  LaunchPlan p;
+  p.width = ix->W;
+  int trav = ix->cfg.traversal;
+  if (trav == RTS_TRAVERSAL_AUTO) trav = (pred == kPoint || ix->W <= 8) ? RTS_TRAVERSAL_THREAD : RTS_TRAVERSAL_TEAM;
+  p.team = (trav == RTS_TRAVERSAL_TEAM);
+  p.chunk = ix->cfg.chunk ? ix->cfg.chunk : (p.team ? 64u : 32u);
+  return p;
+}
+
+int check_handler(int handler, void* arg) {
+  if (handler != RTS_HANDLER_COUNT && handler != RTS_HANDLER_COLLECT)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "unknown handler");
+  if (!arg) return fail(RTS_ERR_INVALID_ARGUMENT, "handler argument is null");
+  return RTS_OK;
+}
+
+int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, void* arg,
+              cudaStream_t s) {
+  int rc = check_handler(handler, arg);
+  if (rc) return rc;
+  if (n == 0 || ix->n_ids == 0) return RTS_OK;  // spatial_index.cuh:354-356
+  if (!q) return fail(RTS_ERR_INVALID_ARGUMENT, "queries is null");
+  if (n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in one call");
+  refresh_forest(ix);
+  if ((rc = buf_reserve(ix->work, sizeof(uint32_t), s, false, 0))) return rc;
+  BatchDesc b{};
+  b.queries = q;
+  b.arg = arg;
+  b.n = static_cast<uint32_t>(n);
+  b.pred = pred;
+  b.mode = handler;
+  b.chunk_begin = 0;
+  b.order = nullptr;
+  LaunchPlan plan = plan_for(ix, pred);
+  uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
+  return launch_queries(ix->forest, plan, &b, nullptr, 1, static_cast<uint32_t>(chunks),
+                        static_cast<uint32_t*>(ix->work.ptr), s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rts_config_default(rts_config* c) {
+  if (!c) return fail(RTS_ERR_INVALID_ARGUMENT, "cfg is null");
+  std::memset(c, 0, sizeof(*c));
+  // rtspatial::Config defaults (spatial_index.cuh:22-37).
+  c->max_geometries = 1000ull * 1000 * 10;
+  c->max_queries = 1000ull * 1000;
+  c->preallocate = 0;
+  c->prefer_fast_build_geom = 0;
+  c->prefer_fast_build_query = 0;
+  c->compact = 0;
+  c->geom_sample_rate = 0.2f;
+  c->query_sample_rate = 0.2f;
+  c->intersect_cost_weight = 0.95f;
+  c->max_geom_samples = 10000;
+  c->max_query_samples = 1000;
+  c->max_parallelism = 512;
+  // This library's structure defaults.
+  c->node_width = 8;
+  c->traversal = RTS_TRAVERSAL_AUTO;
+  c->curve = RTS_CURVE_HILBERT;
+  c->max_trees = 8;
+  c->rebuild_fraction = 0.25f;
+  c->sort_queries = 0;
+  c->rebuild_update_fraction = 0.25f;
+  c->chunk = 0;
+  return RTS_OK;
+}
+
+int rts_create(const rts_config* cfg, rts_index** out) {
+  if (!out) return fail(RTS_ERR_INVALID_ARGUMENT, "out is null");
+  *out = nullptr;
+  rts_config c;
+  if (cfg) c = *cfg; else rts_config_default(&c);
+  if (c.node_width != 4 && c.node_width != 8 && c.node_width != 16 && c.node_width != 32)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "node_width must be 4, 8, 16 or 32");
+  if (c.traversal < 0 || c.traversal > 2) return fail(RTS_ERR_INVALID_ARGUMENT, "bad traversal");
+  if (c.curve != RTS_CURVE_MORTON && c.curve != RTS_CURVE_HILBERT)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "bad curve");
+  if (c.max_trees < 1 || c.max_trees > kMaxTrees)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "max_trees must be in 1..16");
+  auto* ix = new (std::nothrow) rts_index();
+  if (!ix) return fail(RTS_ERR_OUT_OF_MEMORY, "host allocation failed");
+  ix->cfg = c;
+  ix->W = c.node_width;
+  if (c.preallocate && c.max_geometries) {
+    int rc = ensure_slots(ix, round_up(c.max_geometries, kSlotAlign) + kSlotAlign * kMaxTrees, 0);
+    if (!rc) rc = ensure_ids(ix, c.max_geometries, 0);
+    if (rc) {
+      rts_destroy(ix);
+      return rc;
+    }
+  }
+  *out = ix;
+  return RTS_OK;
+}
+
+int rts_destroy(rts_index* ix) {
+  if (!ix) return RTS_OK;
+  cudaStream_t s = 0;
+  bool touched = false;
+  for (auto& t : ix->trees) {
+    touched |= t.nodes.ptr != nullptr;
+    buf_free(t.nodes, s);
+  }
+  DevBuf* all[] = {&ix->leaves, &ix->leaf_ids, &ix->pos, &ix->keys_a, &ix->keys_b, &ix->vals_a,
+                   &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp, &ix->work};
+  for (DevBuf* b : all) {
+    touched |= b->ptr != nullptr;
+    buf_free(*b, s);
+  }
+  ix->staging.release();
+  if (touched) cudaStreamSynchronize(s);  // frees are stream-ordered
+  delete ix;
+  return RTS_OK;
+}
+
+int rts_clear(rts_index* ix, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (auto& t : ix->trees) buf_free(t.nodes, s);
+  ix->trees.clear();
+  ix->n_ids = 0;
+  ix->slot_end = 0;
+  ix->updated_since_build = 0;
+  ix->forest_dirty = true;
+  return RTS_OK;
+}
+
+int rts_insert(rts_index* ix, const float* envelopes, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (n == 0) return RTS_OK;  // spatial_index.cuh:144-146
+  if (!envelopes) return fail(RTS_ERR_INVALID_ARGUMENT, "envelopes is null");
+  if (ix->n_ids + n >= 0xffffffffull)
+    return fail(RTS_ERR_CAPACITY, "ids are 32-bit: at most 2^32-2 envelopes per index");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const auto* src = reinterpret_cast<const float4*>(envelopes);
+  int rc;
+  const uint64_t slot_base = ix->slot_end;
+  const uint64_t slot_end = slot_base + round_up(n, kSlotAlign);
+  if ((rc = ensure_slots(ix, slot_end, s))) return rc;
+  if ((rc = ensure_ids(ix, ix->n_ids + n, s))) return rc;
+  if ((rc = sort_into_slots(ix, src, nullptr, nullptr, n, ix->n_ids, slot_base, leaves_of(ix),
+                            ids_of(ix), s)))
+    return rc;
+  HostTree t;
+  t.id_begin = ix->n_ids;
+  t.n = n;
+  t.slot_base = slot_base;
+  const bool merge = !ix->trees.empty() &&
+                     (static_cast<int>(ix->trees.size()) >= ix->cfg.max_trees ||
+                      static_cast<double>(n) > ix->cfg.rebuild_fraction * static_cast<double>(ix->n_ids));
+  ix->n_ids += n;
+  ix->slot_end = slot_end;
+  ix->forest_dirty = true;
+  if (merge) {
+    ix->trees.push_back(t);  // no levels yet; rebuild_all only reads its slots
+    return rebuild_all(ix, s);
+  }
+  if ((rc = build_tree_levels(ix, t, s))) return rc;
+  ix->trees.push_back(t);
+  return RTS_OK;
+}
+
+int rts_delete(rts_index* ix, const uint64_t* ids, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (n == 0 || ix->n_ids == 0) return RTS_OK;
+  if (!ids) return fail(RTS_ERR_INVALID_ARGUMENT, "ids is null");
+  return launch_delete(ids, n, ix->n_ids, pos_of(ix), leaves_of(ix),
+                       static_cast<cudaStream_t>(stream));
+}
+
+int rts_update(rts_index* ix, const rts_update_entry* upd, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (n == 0 || ix->n_ids == 0) return RTS_OK;
+  if (!upd) return fail(RTS_ERR_INVALID_ARGUMENT, "updates is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = launch_update(upd, n, ix->n_ids, pos_of(ix), leaves_of(ix), s);
+  if (rc) return rc;
+  ix->updated_since_build += n;
+  if (static_cast<double>(ix->updated_since_build) >
+      ix->cfg.rebuild_update_fraction * static_cast<double>(ix->n_ids))
+    return rebuild_all(ix, s);
+  for (auto& t : ix->trees)
+    if ((rc = launch_pack_tree(leaves_of(ix) + t.slot_base, t, ix->W, s))) return rc;
+  return RTS_OK;
+}
+
+int rts_query_points(rts_index* ix, int predicate, const float* points, uint64_t n, int handler,
+                     void* arg, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (predicate != RTS_PREDICATE_CONTAINS)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
+  return query_one(ix, kPoint, points, n, handler, arg, static_cast<cudaStream_t>(stream));
+}
+
+int rts_query_envelopes(rts_index* ix, int predicate, const float* envelopes, uint64_t n,
+                        int handler, void* arg, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  int pred;
+  if (predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
+  else if (predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
+  else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
+  return query_one(ix, pred, envelopes, n, handler, arg, static_cast<cudaStream_t>(stream));
+}
+
+int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batches, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (n_batches == 0) return RTS_OK;
+  if (!batches) return fail(RTS_ERR_INVALID_ARGUMENT, "batches is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  std::vector<BatchDesc> descs;
+  descs.reserve(n_batches);
+  uint64_t chunks = 0;
+  int rc;
+  LaunchPlan plan = plan_for(ix, kContains);
+  for (uint32_t i = 0; i < n_batches; ++i) {
+    const rts_batch& b = batches[i];
+    if ((rc = check_handler(b.handler, b.arg))) return rc;
+    int pred;
+    if (b.query_kind == RTS_QUERY_POINTS) {
+      if (b.predicate != RTS_PREDICATE_CONTAINS)
+        return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
+      pred = kPoint;
+    } else if (b.query_kind == RTS_QUERY_ENVELOPES) {
+      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
+      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
+      else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
+    } else {
+      return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
+    }
+    if (b.n == 0) continue;
+    if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
+    if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
+    BatchDesc d{};
+    d.queries = b.queries;
+    d.arg = b.arg;
+    d.n = static_cast<uint32_t>(b.n);
+    d.pred = pred;
+    d.mode = b.handler;
+    d.chunk_begin = static_cast<uint32_t>(chunks);
+    d.order = nullptr;
+    chunks += (b.n + plan.chunk - 1) / plan.chunk;
+    if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
+    descs.push_back(d);
+  }
+  if (descs.empty() || ix->n_ids == 0) return RTS_OK;
+  refresh_forest(ix);
+  if ((rc = buf_reserve(ix->work, sizeof(uint32_t), s, false, 0))) return rc;
+  void* ddev = nullptr;
+  if (descs.size() > 1 &&
+      (rc = ix->staging.put(descs.data(), descs.size() * sizeof(BatchDesc), s, &ddev)))
+    return rc;
+  return launch_queries(ix->forest, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
+                        static_cast<uint32_t>(descs.size()), static_cast<uint32_t>(chunks),
+                        static_cast<uint32_t*>(ix->work.ptr), s);
+}
+
+uint64_t rts_size(const rts_index* ix) { return ix ? ix->n_ids : 0; }
+
+uint32_t rts_num_trees(const rts_index* ix) {
+  return ix ? static_cast<uint32_t>(ix->trees.size()) : 0;
+}
+
+uint64_t rts_memory_usage(const rts_index* ix) {
+  if (!ix) return 0;
+  uint64_t b = ix->leaves.bytes + ix->leaf_ids.bytes + ix->pos.bytes;
+  for (const auto& t : ix->trees) b += t.nodes.bytes;
+  return b;
+}
+
+const char* rts_last_error(void) { return g_err.c_str(); }
+
+const char* rts_version(void) { return "rtspatial_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// Host-side internals shared by the C-ABI implementation and the launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rts_device.cuh"
+#include "rts_traverse.cuh"
+#include "../../include/rtspatial_b200.h"
+
+namespace rts {
+
+// Per-thread error message behind rts_last_error().
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define RTS_CUDA_TRY(expr)                                 \
+  do {                                                     \
+    cudaError_t _e = (expr);                               \
+    if (_e != cudaSuccess) return ::rts::cuda_fail(_e, #expr); \
+  } while (0)
+
+// Device memory owned by the index (stream-ordered allocator).
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+int buf_reserve(DevBuf& b, size_t bytes, cudaStream_t s, bool keep_contents, size_t used_bytes);
+void buf_free(DevBuf& b, cudaStream_t s);
+
+struct HostTree {
+  uint64_t id_begin = 0;   // ids [id_begin, id_begin + n)
+  uint64_t n = 0;
+  uint64_t slot_base = 0;  // leaves slots [slot_base, slot_base + n)
+  uint32_t top = 0;
+  uint32_t level_off[kMaxLevels] = {};
+  uint32_t level_cnt[kMaxLevels] = {};
+  uint64_t node_entries = 0;
+  DevBuf nodes;
+};
+
+// Level plan of one tree of n envelopes at width W: entries per level and
+// their offsets in the node buffer (entry 0 = root box; levels start at W).
+void plan_levels(uint64_t n, int W, HostTree& t);
+
+// ---- build kernels (rts_build.cu) -----------------------------------------
+// Boxes are read as boxes[idx[i]] when idx is non-null, else boxes[i].
+// bounds: 4 device uint32 (order-preserving encodings of the centre bounds).
+int launch_center_bounds(const float4* boxes, const uint32_t* idx, uint64_t n, uint32_t* bounds,
+                         cudaStream_t s);
+// keys[i] = curve index of the centre of box i; vals[i] = idx ? idx[i] : i.
+int launch_curve_keys(const float4* boxes, const uint32_t* idx, uint64_t n, const uint32_t* bounds,
+                      int curve, uint32_t* keys, uint32_t* vals, cudaStream_t s);
+int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
+               uint64_t n, DevBuf& temp, cudaStream_t s);
+// For i < n with o = order[i]: leaves[slot_base+i] = src[o];
+// id = src_ids ? src_ids[o] : id_begin + o; leaf_ids[slot_base+i] = id;
+// pos[id] = slot_base + i.
+int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
+                  uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
+                  uint32_t* pos, cudaStream_t s);
+// Empty boxes (+inf, +inf, -inf, -inf) in slots [from, to); ids = ~0.
+int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s);
+// Levels 1..top and the root box of a tree from its leaves (also the refit).
+int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_t s);
+// slots[id_begin_t + i] = slot_base_t + i for every tree t; meta (device) =
+// {id_begin, n, slot_base} per tree.
+int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint32_t* slots,
+                     cudaStream_t s);
+int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
+                  float4* leaves, cudaStream_t s);
+int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
+                  float4* leaves, cudaStream_t s);
+
+// ---- query launcher (rts_query.cu) ----------------------------------------
+struct LaunchPlan {
+  int width = 8;
+  bool team = false;
+  uint32_t chunk = 32;  // queries per work item
+};
+// Runs `nb` batches (descriptors in host memory `hb`; device copy `db` when
+// nb > 1) in one persistent launch.  work_counter: zeroed device uint32.
+int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
+                   const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
+                   uint32_t* work_counter, cudaStream_t s);
+// Resident CTAs per SM of the chosen query kernel (for sizing the grid).
+int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks);
+
+}  // namespace rts

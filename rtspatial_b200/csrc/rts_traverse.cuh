@@ -1,0 +1,235 @@
+// Traversal of the implicit W-wide forest, one warp at a time.
+//
+// Two warp-level schemes over the same layout:
+//  - thread: each lane owns one query and tests a whole group of W children
+//    per step (W float4 loads, W predicate evaluations);
+//  - team:   W lanes own one query and each tests one child per step (one
+//    coalesced 16*W-byte load per team, a ballot builds the child mask).
+// Both keep, per query, the child masks of every level on the way down
+// (MaskStack) instead of a pointer stack: descending takes the lowest set bit
+// of the current level's mask; ascending divides the group index by W.
+//
+// A warp works through a chunk [cbeg, cend) of one batch's queries.  Lanes
+// (or teams) whose query is finished take the next unstarted query of the
+// chunk at the end of each step (ballot + popc ranking), so the warp stays
+// full while the chunk lasts even when per-query work is heavily skewed.
+#pragma once
+
+#include "rts_device.cuh"
+
+namespace rts {
+
+// Parameters of one batch (one reference Query call).
+struct BatchDesc {
+  const float* queries;
+  void* arg;              // counter (count) or DevQueue* (collect)
+  uint32_t n;             // queries in the batch
+  int32_t pred;           // PredKind
+  int32_t mode;           // HandlerKind
+  uint32_t chunk_begin;   // index of the batch's first chunk in the launch
+  const uint32_t* order;  // optional visiting order (query ids), or nullptr
+  uint32_t pad[2];
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <int PRED, int W>
+struct TravState {
+  typename QueryOps<PRED>::Q q;
+  MaskStack<W> ms;
+  uint32_t qid;   // id reported for this query
+  uint32_t t;     // tree
+  uint32_t L;     // level of the group being visited
+  uint32_t g;     // group index at level L
+};
+
+// Starts query qid (visiting slot `slot` of the batch) at the top of tree 0.
+// Returns false when the forest is empty.
+template <int PRED, int W>
+__device__ __forceinline__ bool trav_start(const Forest& F, const BatchDesc& B, uint32_t slot,
+                                           TravState<PRED, W>& s) {
+  s.qid = B.order ? B.order[slot] : slot;
+  s.q = QueryOps<PRED>::load(B.queries, s.qid);
+  s.ms.clear();
+  s.t = 0;
+  if (F.n_trees == 0) return false;
+  const TreeDesc& T = F.tree[0];
+  s.L = T.top;
+  s.g = 0;
+  QueryOps<PRED>::enter_tree(s.q, __ldg(T.nodes));
+  return true;
+}
+
+// After a group was visited: moves to the next group to visit.  Returns false
+// when the query is finished in every tree.
+template <int PRED, int W>
+__device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>& s) {
+  for (;;) {
+    uint32_t top = F.tree[s.t].top;
+    while (s.L == 0 || s.ms.get(s.L) == 0) {
+      if (s.L == top) break;
+      s.L += 1;
+      s.g /= W;
+    }
+    if (s.L != 0 && s.ms.get(s.L) != 0) {
+      uint32_t m = s.ms.get(s.L);
+      uint32_t c = __ffs(m) - 1;
+      s.ms.set(s.L, m & (m - 1));
+      s.g = s.g * W + c;
+      s.L -= 1;
+      return true;
+    }
+    // This tree is exhausted: enter the next one at its top group.
+    s.t += 1;
+    if (s.t >= F.n_trees) return false;
+    const TreeDesc& T = F.tree[s.t];
+    s.ms.clear();
+    s.L = T.top;
+    s.g = 0;
+    QueryOps<PRED>::enter_tree(s.q, __ldg(T.nodes));
+    return true;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// thread scheme
+// ---------------------------------------------------------------------------
+template <int PRED, int MODE, int W>
+__device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDesc& B,
+                                                 uint32_t cbeg, uint32_t cend) {
+  using Ops = QueryOps<PRED>;
+  const uint32_t lane = lane_id();
+  TravState<PRED, W> s;
+  uint32_t next = cbeg;
+  bool active = false;
+  {
+    uint32_t slot = next + lane;
+    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+    next = min(cend, next + 32u);
+  }
+  DevQueue qu{};
+  if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
+  unsigned long long cnt = 0;
+
+  while (__any_sync(kFull, active)) {
+    uint32_t leafm = 0;
+    const uint32_t* leafids = nullptr;
+    if (active) {
+      const TreeDesc& T = F.tree[s.t];
+      const uint32_t first = s.g * W;
+      if (s.L == 0) {
+        const float4* p = T.leaves + first;
+        const uint32_t lim = T.n - first;
+        float4 e[W];
+#pragma unroll
+        for (int c = 0; c < W; ++c) e[c] = __ldg(p + c);
+#pragma unroll
+        for (int c = 0; c < W; ++c)
+          if (static_cast<uint32_t>(c) < lim && Ops::leaf(e[c], s.q)) leafm |= 1u << c;
+        leafids = T.ids + first;
+      } else {
+        const float4* p = T.nodes + T.level_off[s.L] + first;
+        const uint32_t lim = T.level_cnt[s.L] - first;
+        float4 e[W];
+#pragma unroll
+        for (int c = 0; c < W; ++c) e[c] = __ldg(p + c);
+        uint32_t m = 0;
+#pragma unroll
+        for (int c = 0; c < W; ++c)
+          if (static_cast<uint32_t>(c) < lim && Ops::node(e[c], s.q)) m |= 1u << c;
+        s.ms.set(s.L, m);
+      }
+    }
+    if (MODE == kCollect) {
+      collect_warp(qu, leafm, leafids, s.qid);
+    } else {
+      cnt += __popc(leafm);
+    }
+    if (active) active = trav_advance<PRED, W>(F, s);
+    // Refill finished lanes from the chunk.
+    uint32_t idle = __ballot_sync(kFull, !active);
+    if (idle != 0 && next < cend) {
+      uint32_t slot = next + __popc(idle & lanemask_lt());
+      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+      next = min(cend, next + __popc(idle));
+    }
+  }
+  if (MODE == kCount) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
+}
+
+// ---------------------------------------------------------------------------
+// team scheme: W lanes per query, 32 / W queries in flight per warp
+// ---------------------------------------------------------------------------
+template <int PRED, int MODE, int W>
+__device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc& B,
+                                               uint32_t cbeg, uint32_t cend) {
+  using Ops = QueryOps<PRED>;
+  constexpr uint32_t kTeams = 32 / W;
+  constexpr uint32_t kTeamMask = (W == 32) ? kFull : ((1u << W) - 1u);
+  const uint32_t lane = lane_id();
+  const uint32_t team = lane / W;
+  const uint32_t tl = lane % W;
+  TravState<PRED, W> s;
+  uint32_t next = cbeg;
+  bool active = false;
+  {
+    uint32_t slot = next + team;
+    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+    next = min(cend, next + kTeams);
+  }
+  DevQueue qu{};
+  if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
+  unsigned long long cnt = 0;
+
+  while (__any_sync(kFull, active)) {
+    bool hit = false, leaf_hit = false;
+    uint32_t gid = 0;
+    if (active) {
+      const TreeDesc& T = F.tree[s.t];
+      const uint32_t first = s.g * W;
+      if (s.L == 0) {
+        float4 e = __ldg(T.leaves + first + tl);
+        hit = (first + tl < T.n) && Ops::leaf(e, s.q);
+        leaf_hit = hit;
+        if (leaf_hit) gid = __ldg(T.ids + first + tl);
+      } else {
+        float4 e = __ldg(T.nodes + T.level_off[s.L] + first + tl);
+        hit = (first + tl < T.level_cnt[s.L]) && Ops::node(e, s.q);
+      }
+    }
+    const uint32_t bal = __ballot_sync(kFull, hit);
+    const uint32_t leafbal = __ballot_sync(kFull, leaf_hit);
+    if (MODE == kCollect) {
+      if (leafbal) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(qu.size, static_cast<uint32_t>(__popc(leafbal)));
+        base = __shfl_sync(kFull, base, 0);
+        if (leaf_hit) {
+          unsigned long long p = static_cast<unsigned long long>(base) + __popc(leafbal & lanemask_lt());
+          if (p < qu.capacity) qu.data[p] = DevPair{gid, s.qid};
+        }
+      }
+    } else {
+      cnt += leaf_hit ? 1u : 0u;
+    }
+    if (active) {
+      if (s.L != 0) s.ms.set(s.L, (bal >> (team * W)) & kTeamMask);
+      active = trav_advance<PRED, W>(F, s);
+    }
+    // Refill finished teams from the chunk (all lanes of a team agree).
+    uint32_t idle = __ballot_sync(kFull, !active);
+    if (idle != 0 && next < cend) {
+      uint32_t below = (team == 0) ? 0u : (idle & ((1u << (team * W)) - 1u));
+      uint32_t slot = next + __popc(below) / W;
+      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+      next = min(cend, next + __popc(idle) / W);
+    }
+  }
+  if (MODE == kCount) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
+}
+
+}  // namespace rts
