@@ -72,10 +72,11 @@ def make_workload(cfg: int, scale: float, rank: int):
     from rtspatial_b200 import workloads as wl
     if cfg == 2:
         nb, nq = int(10_000_000 * scale), int(1_000_000 * scale)
-        boxes, _, _ = wl.config2(seed=42, n_boxes=nb, n_queries=16)
-        rng = np.random.default_rng(1000 + rank)
-        queries = wl.uniform_boxes(rng, nq, 1e-3)
-        sizes = wl.log_uniform_sizes(rng, 256, 1024, 16384, nq)
+        boxes, queries, sizes = wl.config2(seed=42, n_boxes=nb, n_queries=nq)
+        if rank:
+            rng = np.random.default_rng(1000 + rank)
+            queries = wl.uniform_boxes(rng, nq, 1e-3)
+            sizes = wl.log_uniform_sizes(rng, 256, 1024, 16384, nq)
         desc = (f"range-contains: {nb} boxes (64 Gaussian clusters, sigma 0.02, sides U[0,5e-3]) x "
                 f"{nq} query boxes (uniform, sides U[0,1e-3]) in 256 log-uniform batches "
                 f"[1K,16K], one persistent launch, collecting handler")

@@ -62,13 +62,26 @@ def log_uniform_sizes(rng: np.random.Generator, n_batches: int, lo: int, hi: int
                       total: int | None = None) -> np.ndarray:
     """Batch sizes log-uniform in [lo, hi]; rescaled to sum to `total`."""
     s = np.exp(rng.uniform(np.log(lo), np.log(hi), n_batches))
-    if total is not None:
-        s = s * (total / s.sum())
-    s = np.maximum(np.round(s).astype(np.int64), 1)
-    if total is not None:
-        s[-1] += total - s.sum()
-        assert s[-1] >= 1
-    return s
+    if total is None:
+        return np.maximum(np.round(s).astype(np.int64), 1)
+    assert total >= n_batches
+    s = s * (total / s.sum())
+    out = np.maximum(np.floor(s).astype(np.int64), 1)
+    # hand out the remainder by largest fractional part (largest remainder)
+    rest = total - int(out.sum())
+    frac = s - np.floor(s)
+    order = np.argsort(-frac, kind="stable")
+    i = 0
+    while rest > 0:
+        out[order[i % n_batches]] += 1
+        rest -= 1
+        i += 1
+    while rest < 0:
+        j = int(np.argmax(out))
+        out[j] -= 1
+        rest += 1
+    assert out.sum() == total and out.min() >= 1
+    return out
 
 
 # ---- the five configurations --------------------------------------------
