@@ -1,0 +1,160 @@
+// rtspatial::SpatialIndex<float, 2> on the B200 library.
+//
+// Same class, method names, argument types and asynchrony as the reference's
+// public API; every call forwards to the C-ABI in rtspatial_b200.h and throws
+// rtspatial::Exception on failure.  Link with -lrtspatial_b200.
+//
+// Handlers.  The reference picks its per-pair device handler when its shaders
+// are compiled (counting or collecting header).  Here Config::handler picks
+// one of the same two behaviours at run time; its default follows the macro
+// RTSPATIAL_COUNTING_HANDLERS (defined: counting, arg = unsigned long long*;
+// otherwise collecting, arg = dev::Queue<thrust::pair<uint32_t,uint32_t>>* in
+// device memory).
+#ifndef RTSPATIAL_B200_SPATIAL_INDEX_CUH
+#define RTSPATIAL_B200_SPATIAL_INDEX_CUH
+
+#include <thrust/pair.h>
+
+#include <cstdint>
+#include <iostream>
+#include <string>
+#include <type_traits>
+
+#include "rtspatial/geom/envelope.cuh"
+#include "rtspatial/geom/point.cuh"
+#include "rtspatial/geom/predicates.h"
+#include "rtspatial/utils/array_view.h"
+#include "rtspatial/utils/exception.h"
+#include "rtspatial/utils/queue.h"
+#include "rtspatial_b200.h"
+
+#ifdef RTSPATIAL_COUNTING_HANDLERS
+#define RTSPATIAL_DEFAULT_HANDLER RTS_HANDLER_COUNT
+#else
+#define RTSPATIAL_DEFAULT_HANDLER RTS_HANDLER_COLLECT
+#endif
+
+namespace rtspatial {
+
+struct Config {
+  std::string ptx_root;  // no PTX modules to load; kept for source compatibility
+  size_t max_geometries = 1000 * 1000 * 10;
+  size_t max_queries = 1000 * 1000;
+  bool preallocate = false;
+  bool prefer_fast_build_geom = false;
+  bool prefer_fast_build_query = false;
+  bool compact = false;
+  float geom_sample_rate = 0.2;
+  float query_sample_rate = 0.2;
+  float intersect_cost_weight = 0.95;
+  uint32_t max_geom_samples = 10000;
+  uint32_t max_query_samples = 1000;
+  uint32_t max_parallelism = 512;
+  // B200 library knobs
+  int handler = RTSPATIAL_DEFAULT_HANDLER;
+  int node_width = 8;
+  int traversal = RTS_TRAVERSAL_AUTO;
+  int curve = RTS_CURVE_HILBERT;
+  int max_trees = 8;
+  float rebuild_fraction = 0.25f;
+  float rebuild_update_fraction = 0.25f;
+  uint32_t chunk = 0;
+};
+
+template <typename COORD_T, int N_DIMS>
+class SpatialIndex {
+  static_assert(std::is_same<COORD_T, float>::value && N_DIMS == 2,
+                "the B200 library indexes float 2-D envelopes");
+
+ public:
+  using point_t = Point<COORD_T, N_DIMS>;
+  using envelope_t = Envelope<point_t>;
+
+  SpatialIndex() = default;
+  SpatialIndex(const SpatialIndex&) = delete;
+  SpatialIndex& operator=(const SpatialIndex&) = delete;
+  ~SpatialIndex() {
+    if (h_) rts_destroy(h_);
+  }
+
+  void Init(const Config& config) {
+    config_ = config;
+    rts_config c;
+    RTS_CHECK(rts_config_default(&c));
+    c.max_geometries = config.max_geometries;
+    c.max_queries = config.max_queries;
+    c.preallocate = config.preallocate;
+    c.prefer_fast_build_geom = config.prefer_fast_build_geom;
+    c.prefer_fast_build_query = config.prefer_fast_build_query;
+    c.compact = config.compact;
+    c.geom_sample_rate = config.geom_sample_rate;
+    c.query_sample_rate = config.query_sample_rate;
+    c.intersect_cost_weight = config.intersect_cost_weight;
+    c.max_geom_samples = config.max_geom_samples;
+    c.max_query_samples = config.max_query_samples;
+    c.max_parallelism = config.max_parallelism;
+    c.node_width = config.node_width;
+    c.traversal = config.traversal;
+    c.curve = config.curve;
+    c.max_trees = config.max_trees;
+    c.rebuild_fraction = config.rebuild_fraction;
+    c.rebuild_update_fraction = config.rebuild_update_fraction;
+    c.chunk = config.chunk;
+    if (h_) rts_destroy(h_);
+    h_ = nullptr;
+    RTS_CHECK(rts_create(&c, &h_));
+  }
+
+  void Clear() { RTS_CHECK(rts_clear(handle(), nullptr)); }
+
+  void Insert(ArrayView<envelope_t> envelopes, cudaStream_t stream = nullptr) {
+    RTS_CHECK(rts_insert(handle(), reinterpret_cast<const float*>(envelopes.data()),
+                         envelopes.size(), stream));
+  }
+
+  void Delete(const ArrayView<size_t> ids, cudaStream_t stream) {
+    static_assert(sizeof(size_t) == 8, "64-bit ids");
+    RTS_CHECK(rts_delete(handle(), reinterpret_cast<const uint64_t*>(ids.data()), ids.size(),
+                         stream));
+  }
+
+  void Update(const ArrayView<thrust::pair<size_t, envelope_t>> updates, cudaStream_t stream) {
+    static_assert(sizeof(thrust::pair<size_t, envelope_t>) == sizeof(rts_update_entry),
+                  "update records are {size_t id; envelope}");
+    RTS_CHECK(rts_update(handle(), reinterpret_cast<const rts_update_entry*>(updates.data()),
+                         updates.size(), stream));
+  }
+
+  void Query(Predicate p, ArrayView<point_t> queries, void* arg,
+             cudaStream_t stream = nullptr) {
+    RTS_CHECK(rts_query_points(handle(), static_cast<int>(p),
+                               reinterpret_cast<const float*>(queries.data()), queries.size(),
+                               config_.handler, arg, stream));
+  }
+
+  void Query(Predicate p, ArrayView<envelope_t> queries, void* arg,
+             cudaStream_t stream = nullptr) {
+    RTS_CHECK(rts_query_envelopes(handle(), static_cast<int>(p),
+                                  reinterpret_cast<const float*>(queries.data()), queries.size(),
+                                  config_.handler, arg, stream));
+  }
+
+  size_t size() const { return h_ ? rts_size(h_) : 0; }
+
+  void PrintMemoryUsage() {
+    std::cout << "Index " << rts_memory_usage(handle()) / 1024 / 1024 << " MB" << std::endl;
+  }
+
+  rts_index* native_handle() { return h_; }
+
+ private:
+  rts_index* handle() {
+    if (!h_) throw Exception("SpatialIndex used before Init()");
+    return h_;
+  }
+  Config config_;
+  rts_index* h_ = nullptr;
+};
+
+}  // namespace rtspatial
+#endif
