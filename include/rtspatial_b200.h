@@ -182,6 +182,22 @@ typedef struct rts_batch {
 int rts_query_batched(rts_index* index, const rts_batch* batches, uint32_t n_batches,
                       void* stream);
 
+/* No counterpart in the reference.  The same as rts_query_batched, but it
+ * allocates no memory: for callers that cannot call cudaMalloc once they are
+ * serving (HBM reserved up front, allocation forbidden on the request path,
+ * buffers only from the host engine's own memory manager).  Its scratch — the
+ * device work counter and the device copy of the batch descriptors — is a
+ * fixed array in the library (about 49 KB per device that loads it, held until
+ * the process exits) instead of index-owned buffers.  At most
+ * RTS_NOALLOC_MAX_BATCHES non-empty batches per call (RTS_ERR_CAPACITY
+ * otherwise).  All calls on a device share that array: calls that overlap on
+ * the GPU race.  The first call on a device looks up the array's device
+ * address; make it before any stream capture.  The index must already be
+ * built; inputs and outputs are the caller's, as in rts_query_batched. */
+#define RTS_NOALLOC_MAX_BATCHES 1024
+int rts_query_batched_noalloc(rts_index* index, const rts_batch* batches, uint32_t n_batches,
+                              void* stream);
+
 /* ---- introspection ------------------------------------------------------ */
 uint64_t rts_size(const rts_index* index);       /* number of ids handed out */
 uint32_t rts_num_trees(const rts_index* index);  /* sub-trees currently indexed */

@@ -31,6 +31,7 @@ RTS_CURVE_MORTON = 0
 RTS_CURVE_HILBERT = 1
 RTS_QUERY_POINTS = 0
 RTS_QUERY_ENVELOPES = 1
+RTS_NOALLOC_MAX_BATCHES = 1024
 
 
 class rts_config(ctypes.Structure):
@@ -94,6 +95,7 @@ SIGNATURES = {
     "rts_query_points": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
     "rts_query_envelopes": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
     "rts_query_batched": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
+    "rts_query_batched_noalloc": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_size": (_U64, [_P]),
     "rts_num_trees": (ctypes.c_uint32, [_P]),
     "rts_memory_usage": (_U64, [_P]),

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -555,3 +556,114 @@ const char* rts_last_error(void) { return g_err.c_str(); }
 const char* rts_version(void) { return "rtspatial_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched query that allocates nothing.
+//
+// For callers that must not allocate device memory once they are serving:
+// processes that reserve HBM for the index and its buffers at start-up and
+// forbid cudaMalloc on the request path (cudaMalloc can synchronize the
+// device and its latency is unbounded), host engines that hand this library
+// only buffers from their own memory manager, and real-time loops that cannot
+// take an allocation failure mid-request.  rts_query_batched keeps its work
+// counter and the device copy of the batch descriptors in index-owned device
+// buffers that it grows on demand; this variant keeps both in a file-scope
+// device array of fixed size instead.
+//
+// The array exists once per device that loads the library and lives until the
+// process exits.  Every call on a device uses the same array: the work
+// counter is cleared by each call, the descriptor area keeps the previous
+// call's contents, and calls that overlap on the GPU (other streams, other
+// threads, other indexes) race on it.  The first call on a device looks up
+// the array's device address (cudaGetSymbolAddress); make that first call
+// before any stream capture.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr uint32_t kNoAllocMaxBatches = RTS_NOALLOC_MAX_BATCHES;
+constexpr size_t kNoAllocCounterBytes = 256;
+constexpr size_t kNoAllocBytes = kNoAllocCounterBytes + kNoAllocMaxBatches * sizeof(BatchDesc);
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once
+// per device; the array's name is only a host-side stand-in).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  RTS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(RTS_ERR_UNSUPPORTED, "device ordinal beyond the no-allocation table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return RTS_OK;
+}
+}  // namespace
+
+extern "C" int rts_query_batched_noalloc(rts_index* ix, const rts_batch* batches,
+                                         uint32_t n_batches, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (n_batches == 0) return RTS_OK;
+  if (!batches) return fail(RTS_ERR_INVALID_ARGUMENT, "batches is null");
+  if (n_batches > kNoAllocMaxBatches)
+    return fail(RTS_ERR_CAPACITY, "rts_query_batched_noalloc takes at most " +
+                                      std::to_string(kNoAllocMaxBatches) + " batches, got " +
+                                      std::to_string(n_batches));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BatchDesc descs[kNoAllocMaxBatches];
+  uint32_t nd = 0;
+  uint64_t chunks = 0;
+  int rc;
+  LaunchPlan plan = plan_for(ix, kContains);
+  for (uint32_t i = 0; i < n_batches; ++i) {
+    const rts_batch& b = batches[i];
+    if ((rc = check_handler(b.handler, b.arg))) return rc;
+    int pred;
+    if (b.query_kind == RTS_QUERY_POINTS) {
+      if (b.predicate != RTS_PREDICATE_CONTAINS)
+        return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
+      pred = kPoint;
+    } else if (b.query_kind == RTS_QUERY_ENVELOPES) {
+      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
+      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
+      else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
+    } else {
+      return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
+    }
+    if (b.n == 0) continue;
+    if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
+    if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
+    BatchDesc& d = descs[nd++];
+    d = BatchDesc{};
+    d.queries = b.queries;
+    d.arg = b.arg;
+    d.n = static_cast<uint32_t>(b.n);
+    d.pred = pred;
+    d.mode = b.handler;
+    d.chunk_begin = static_cast<uint32_t>(chunks);
+    d.order = nullptr;
+    chunks += (b.n + plan.chunk - 1) / plan.chunk;
+    if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
+  }
+  if (nd == 0 || ix->n_ids == 0) return RTS_OK;
+  void* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  refresh_forest(ix);
+  auto* counter = static_cast<uint32_t*>(scratch);
+  auto* ddescs = reinterpret_cast<BatchDesc*>(static_cast<unsigned char*>(scratch) +
+                                              kNoAllocCounterBytes);
+  if (nd > 1)
+    RTS_CUDA_TRY(cudaMemcpyAsync(ddescs, descs, nd * sizeof(BatchDesc), cudaMemcpyHostToDevice, s));
+  return launch_queries(ix->forest, plan, descs, ddescs, nd, static_cast<uint32_t>(chunks),
+                        counter, s);
+}
