@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--traversal", type=int, default=-1)
     ap.add_argument("--curve", type=int, default=-1)
     ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--sort", type=int, default=-1, help="sort_queries: 0 never, 1 always, 2 auto")
+    ap.add_argument("--occupancy", type=int, default=-1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -126,7 +128,7 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -287,6 +289,10 @@ def main():
         cfg.curve = args.curve
     if args.chunk:
         cfg.chunk = args.chunk
+    if args.sort >= 0:
+        cfg.sort_queries = args.sort
+    if args.occupancy >= 0:
+        cfg.query_occupancy = args.occupancy
     ix = rb.SpatialIndex(cfg)
     boxes_d = torch.from_numpy(w["boxes"]).to(dev)
     torch.cuda.synchronize()
@@ -452,7 +458,8 @@ def main():
                 "workload": w["desc"],
                 "boxes": int(w["boxes"].shape[0]), "queries": nq, "batches": nbatch,
                 "node_width": ix.config.node_width, "traversal": ix.config.traversal,
-                "curve": ix.config.curve,
+                "curve": ix.config.curve, "sort_queries": ix.config.sort_queries,
+                "query_occupancy": ix.config.query_occupancy, "chunk": ix.config.chunk,
                 "l2": "flushed before every timed step (256 MiB write outside the events)",
             },
             "pairs_per_s": total_pairs * world / (step_ms / 1000),

@@ -59,6 +59,8 @@ struct Config {
   float rebuild_fraction = 0.25f;
   float rebuild_update_fraction = 0.25f;
   uint32_t chunk = 0;
+  int sort_queries = 2;
+  int query_occupancy = 0;
 };
 
 template <typename COORD_T, int N_DIMS>
@@ -100,6 +102,8 @@ class SpatialIndex {
     c.rebuild_fraction = config.rebuild_fraction;
     c.rebuild_update_fraction = config.rebuild_update_fraction;
     c.chunk = config.chunk;
+    c.sort_queries = config.sort_queries;
+    c.query_occupancy = config.query_occupancy;
     if (h_) rts_destroy(h_);
     h_ = nullptr;
     RTS_CHECK(rts_create(&c, &h_));

@@ -106,10 +106,13 @@ typedef struct rts_config {
   int32_t curve;          /* RTS_CURVE_*: the order leaves are packed in */
   int32_t max_trees;      /* insert batches kept as separate sub-trees before a merge rebuild (1..16) */
   float rebuild_fraction; /* an insert batch larger than this fraction of the index rebuilds everything */
-  int32_t sort_queries;   /* 1: visit queries in curve order (results keep the caller's query ids) */
+  int32_t sort_queries;   /* visit queries in curve order (results keep the caller's query ids):
+                             0 never, 1 always, 2 when a launch has >= 8192 queries */
   float rebuild_update_fraction; /* updates since the last rebuild, as a fraction of the index,
                                     above which Update re-sorts instead of refitting */
   uint32_t chunk;         /* queries per device work item (0 = library default) */
+  int32_t query_occupancy; /* 0 library default; 4: query kernel capped at 64 registers */
+  int32_t reserved0;
 } rts_config;
 
 #define RTS_TRAVERSAL_AUTO 0
@@ -181,6 +184,22 @@ typedef struct rts_batch {
  * staged by the library; the call returns once they are enqueued. */
 int rts_query_batched(rts_index* index, const rts_batch* batches, uint32_t n_batches,
                       void* stream);
+
+/* ---- prepared launches and CUDA-graph replay -----------------------------
+ * No counterpart in the reference (its Query re-packs launch parameters on
+ * every call, spatial_index.cuh:359-367).  A plan fixes a set of batches
+ * (query pointers, sizes, handlers, outputs): descriptors are validated and
+ * staged once and all launch scratch is sized, so rts_plan_launch only
+ * enqueues kernels and memsets.  With use_graph != 0 the first launch captures
+ * that sequence into a CUDA graph and later launches replay it; Insert, a
+ * rebuild or Clear of the index make the next launch re-capture.  Query data
+ * and output buffers may be rewritten between launches; their sizes may not.
+ * A plan must be destroyed before its index. */
+typedef struct rts_plan rts_plan;
+int rts_plan_create(rts_index* index, const rts_batch* batches, uint32_t n_batches,
+                    rts_plan** out);
+int rts_plan_launch(rts_plan* plan, void* stream, int use_graph);
+int rts_plan_destroy(rts_plan* plan);
 
 /* No counterpart in the reference.  The same as rts_query_batched, but it
  * allocates no memory: for callers that cannot call cudaMalloc once they are

@@ -12,11 +12,12 @@ from .spatial_index import (  # noqa: F401
     Config,
     Counter,
     Handler,
+    Plan,
     Predicate,
     Queue,
     SpatialIndex,
     sort_pairs,
 )
 
-__all__ = ["Config", "Counter", "Handler", "Predicate", "Queue", "SpatialIndex", "sort_pairs",
+__all__ = ["Config", "Counter", "Handler", "Plan", "Predicate", "Queue", "SpatialIndex", "sort_pairs",
            "RtsError", "lib", "LIB_PATH"]

@@ -56,6 +56,8 @@ class rts_config(ctypes.Structure):
         ("sort_queries", ctypes.c_int32),
         ("rebuild_update_fraction", ctypes.c_float),
         ("chunk", ctypes.c_uint32),
+        ("query_occupancy", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
     ]
 
 
@@ -96,6 +98,9 @@ SIGNATURES = {
     "rts_query_envelopes": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
     "rts_query_batched": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_query_batched_noalloc": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
+    "rts_plan_create": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, ctypes.POINTER(_P)]),
+    "rts_plan_launch": (_I, [_P, _P, _I]),
+    "rts_plan_destroy": (_I, [_P]),
     "rts_size": (_U64, [_P]),
     "rts_num_trees": (ctypes.c_uint32, [_P]),
     "rts_memory_usage": (_U64, [_P]),

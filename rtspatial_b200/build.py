@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librtspatial_b200.so")
-SOURCES = ["rts_index.cu", "rts_query.cu", "rts_build.cu"]
-HEADERS = ["rts_device.cuh", "rts_traverse.cuh", "rts_internal.h"]
+SOURCES = ["rts_index.cu", "rts_plan.cu", "rts_query.cu", "rts_build.cu"]
+HEADERS = ["rts_device.cuh", "rts_traverse.cuh", "rts_internal.h", "rts_index_impl.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

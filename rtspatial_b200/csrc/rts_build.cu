@@ -182,6 +182,42 @@ __global__ void k_update(const rts_update_entry* __restrict__ upd, uint64_t n, u
   leaves[pos[e.id]] = make_float4(e.min_x, e.min_y, e.max_x, e.max_y);
 }
 
+// Visiting order of queries: key = (batch index << 32) | curve index of the
+// query's centre in the frame of the first sub-tree's root box; value = the
+// query's index within its batch.  Sorting by key groups batches and, within
+// a batch, puts queries that walk the same nodes next to each other.
+__global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDesc b0, uint32_t nb,
+                             uint64_t total, const float4* __restrict__ frame_box, int curve,
+                             unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  uint32_t b = 0;
+  if (nb > 1) {
+    uint32_t lo = 0, hi = nb - 1;  // largest b with qbase <= i
+    while (lo < hi) {
+      uint32_t mid = (lo + hi + 1) >> 1;
+      if (descs[mid].qbase <= i) lo = mid; else hi = mid - 1;
+    }
+    b = lo;
+  }
+  const BatchDesc& B = (nb > 1) ? descs[b] : b0;
+  const uint32_t local = static_cast<uint32_t>(i - B.qbase);
+  float2 c;
+  if (B.pred == kPoint) {
+    c = reinterpret_cast<const float2*>(B.queries)[local];
+  } else {
+    c = center(reinterpret_cast<const float4*>(B.queries)[local]);
+  }
+  const float4 f = *frame_box;
+  const float sx = (f.z > f.x) ? 65535.0f / (f.z - f.x) : 0.0f;
+  const float sy = (f.w > f.y) ? 65535.0f / (f.w - f.y) : 0.0f;
+  uint32_t qx = __float2uint_rz(fminf(fmaxf((c.x - f.x) * sx, 0.0f), 65535.0f));
+  uint32_t qy = __float2uint_rz(fminf(fmaxf((c.y - f.y) * sy, 0.0f), 65535.0f));
+  uint32_t k = (curve == RTS_CURVE_HILBERT) ? hilbert16(qx, qy) : (spread16(qx) | (spread16(qy) << 1));
+  keys[i] = (static_cast<unsigned long long>(b) << 32) | k;
+  vals[i] = local;
+}
+
 inline unsigned grid_for(uint64_t n) {
   uint64_t g = div_up(n, kThreads);
   return static_cast<unsigned>(g ? g : 1);
@@ -285,6 +321,37 @@ int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint
   dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(n_trees));
   k_slot_list<<<grid, kThreads, 0, s>>>(meta_dev, n_trees, slots);
   RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
+                       const float4* frame_box, int curve, unsigned long long* keys_a,
+                       unsigned long long* keys_b, uint32_t* vals_a, uint32_t* order,
+                       DevBuf& temp, cudaStream_t s) {
+  if (total == 0) return RTS_OK;
+  k_query_keys<<<grid_for(total), kThreads, 0, s>>>(descs, b0, nb, total, frame_box, curve, keys_a,
+                                                    vals_a);
+  RTS_CUDA_TRY(cudaGetLastError());
+  int end_bit = 32;
+  while (end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
+  size_t need = 0;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, keys_a, keys_b, vals_a, order,
+                                                static_cast<int>(total), 0, end_bit, s));
+  int rc = buf_reserve(temp, need, s, false, 0);
+  if (rc) return rc;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.ptr, need, keys_a, keys_b, vals_a, order,
+                                                static_cast<int>(total), 0, end_bit, s));
+  return RTS_OK;
+}
+
+int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes) {
+  int end_bit = 32;
+  while (end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
+  *bytes = 0;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(
+      nullptr, *bytes, static_cast<const unsigned long long*>(nullptr),
+      static_cast<unsigned long long*>(nullptr), static_cast<const uint32_t*>(nullptr),
+      static_cast<uint32_t*>(nullptr), static_cast<int>(total), 0, end_bit));
   return RTS_OK;
 }
 

@@ -17,7 +17,7 @@
 #include <string>
 #include <vector>
 
-#include "rts_internal.h"
+#include "rts_index_impl.h"
 
 namespace rts {
 
@@ -58,8 +58,6 @@ void buf_free(DevBuf& b, cudaStream_t s) {
   b.bytes = 0;
 }
 
-static inline uint64_t round_up(uint64_t a, uint64_t b) { return (a + b - 1) / b * b; }
-
 // Levels storable by the traversal's mask stack at each width.
 static uint32_t max_levels_for(int W) {
   switch (W) {
@@ -71,76 +69,11 @@ static uint32_t max_levels_for(int W) {
   return 0;
 }
 
-// Pinned staging for small host->device copies that must not block the host:
-// a ring of slots, each reused only after the copy that last read it is done.
-struct Staging {
-  static constexpr int kSlots = 4;
-  void* host[kSlots] = {};
-  DevBuf dev[kSlots];
-  size_t host_bytes[kSlots] = {};
-  cudaEvent_t done[kSlots] = {};
-  int next = 0;
-
-  // Copies `bytes` from src to a device buffer; returns its device address.
-  int put(const void* src, size_t bytes, cudaStream_t s, void** dev_out) {
-    int k = next;
-    next = (next + 1) % kSlots;
-    if (done[k]) RTS_CUDA_TRY(cudaEventSynchronize(done[k]));
-    else RTS_CUDA_TRY(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
-    if (host_bytes[k] < bytes) {
-      if (host[k]) cudaFreeHost(host[k]);
-      host[k] = nullptr;
-      size_t cap = std::max<size_t>(bytes, 4096);
-      RTS_CUDA_TRY(cudaMallocHost(&host[k], cap));
-      host_bytes[k] = cap;
-    }
-    int rc = buf_reserve(dev[k], bytes, s, false, 0);
-    if (rc) return rc;
-    std::memcpy(host[k], src, bytes);
-    RTS_CUDA_TRY(cudaMemcpyAsync(dev[k].ptr, host[k], bytes, cudaMemcpyHostToDevice, s));
-    RTS_CUDA_TRY(cudaEventRecord(done[k], s));
-    *dev_out = dev[k].ptr;
-    return RTS_OK;
-  }
-  void release() {
-    for (int k = 0; k < kSlots; ++k) {
-      if (done[k]) {
-        cudaEventSynchronize(done[k]);
-        cudaEventDestroy(done[k]);
-        done[k] = nullptr;
-      }
-      if (host[k]) cudaFreeHost(host[k]);
-      host[k] = nullptr;
-      host_bytes[k] = 0;
-      buf_free(dev[k], 0);
-    }
-  }
-};
-
 }  // namespace rts
 
 using namespace rts;
 
-struct rts_index {
-  rts_config cfg{};
-  int W = 8;
-  uint64_t n_ids = 0;
-  uint64_t slot_end = 0;        // slots in use (each sub-tree padded to 32)
-  uint64_t updated_since_build = 0;
-  DevBuf leaves, leaf_ids, pos;
-  std::vector<HostTree> trees;
-  // scratch of the build path
-  DevBuf keys_a, keys_b, vals_a, vals_b, sort_temp, bounds, slots_tmp;
-  // scratch of the query path
-  DevBuf work;
-  Staging staging;
-  Forest forest{};
-  bool forest_dirty = true;
-};
-
-namespace {
-
-constexpr uint64_t kSlotAlign = 32;
+namespace rts {
 
 int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
   uint64_t need = slots + kSlotAlign;
@@ -252,6 +185,7 @@ int rebuild_all(rts_index* ix, cudaStream_t s) {
   ix->trees.push_back(t);
   ix->updated_since_build = 0;
   ix->forest_dirty = true;
+  ix->version++;
   return RTS_OK;
 }
 
@@ -284,7 +218,86 @@ LaunchPlan plan_for(const rts_index* ix, int pred) {
   if (trav == RTS_TRAVERSAL_AUTO) trav = (pred == kPoint || ix->W <= 8) ? RTS_TRAVERSAL_THREAD : RTS_TRAVERSAL_TEAM;
   p.team = (trav == RTS_TRAVERSAL_TEAM);
   p.chunk = ix->cfg.chunk ? ix->cfg.chunk : (p.team ? 64u : 32u);
+  p.high_occupancy = ix->cfg.query_occupancy >= 4;
   return p;
+}
+
+bool want_sort(const rts_index* ix, uint64_t total) {
+  if (ix->cfg.sort_queries == 0) return false;
+  if (ix->cfg.sort_queries == 1) return true;
+  return total >= 8192;  // auto: small launches are latency-bound, skip the sort
+}
+
+// Assigns each batch its slice of the launch's visiting order (qbase, order)
+// and reserves the sort scratch.  Call before the descriptors are staged.
+int plan_order(QueryScratch& qs, BatchDesc* descs, uint32_t nd, uint64_t total, cudaStream_t s) {
+  int rc;
+  if ((rc = buf_reserve(qs.keys_a, total * 8, s, false, 0))) return rc;
+  if ((rc = buf_reserve(qs.keys_b, total * 8, s, false, 0))) return rc;
+  if ((rc = buf_reserve(qs.vals, total * 4, s, false, 0))) return rc;
+  if ((rc = buf_reserve(qs.order, total * 4, s, false, 0))) return rc;
+  uint64_t q = 0;
+  for (uint32_t i = 0; i < nd; ++i) {
+    descs[i].qbase = static_cast<uint32_t>(q);
+    descs[i].order = static_cast<const uint32_t*>(qs.order.ptr) + q;
+    q += descs[i].n;
+  }
+  return RTS_OK;
+}
+
+// Fills the visiting order planned by plan_order (descriptors already on the
+// device when nd > 1).
+int fill_order(rts_index* ix, QueryScratch& qs, const BatchDesc* host, const BatchDesc* dev,
+               uint32_t nd, uint64_t total, cudaStream_t s) {
+  return launch_query_order(dev, host[0], nd, total,
+                            static_cast<const float4*>(ix->trees[0].nodes.ptr), ix->cfg.curve,
+                            static_cast<unsigned long long*>(qs.keys_a.ptr),
+                            static_cast<unsigned long long*>(qs.keys_b.ptr),
+                            static_cast<uint32_t*>(qs.vals.ptr),
+                            static_cast<uint32_t*>(qs.order.ptr), qs.sort_temp, s);
+}
+
+// Turns public batch descriptions into launch descriptors (validating them);
+// empty batches are dropped.  chunks = work items of the launch.
+int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
+               const LaunchPlan& plan, std::vector<BatchDesc>& out, uint64_t& chunks) {
+  out.clear();
+  out.reserve(n_batches);
+  chunks = 0;
+  int rc;
+  (void)ix;
+  for (uint32_t i = 0; i < n_batches; ++i) {
+    const rts_batch& b = batches[i];
+    if ((rc = check_handler(b.handler, b.arg))) return rc;
+    int pred;
+    if (b.query_kind == RTS_QUERY_POINTS) {
+      if (b.predicate != RTS_PREDICATE_CONTAINS)
+        return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
+      pred = kPoint;
+    } else if (b.query_kind == RTS_QUERY_ENVELOPES) {
+      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
+      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
+      else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
+    } else {
+      return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
+    }
+    if (b.n == 0) continue;
+    if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
+    if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
+    BatchDesc d{};
+    d.queries = b.queries;
+    d.arg = b.arg;
+    d.n = static_cast<uint32_t>(b.n);
+    d.pred = pred;
+    d.mode = b.handler;
+    d.chunk_begin = static_cast<uint32_t>(chunks);
+    d.order = nullptr;
+    d.qbase = 0;
+    chunks += (b.n + plan.chunk - 1) / plan.chunk;
+    if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
+    out.push_back(d);
+  }
+  return RTS_OK;
 }
 
 int check_handler(int handler, void* arg) {
@@ -302,7 +315,7 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   if (!q) return fail(RTS_ERR_INVALID_ARGUMENT, "queries is null");
   if (n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in one call");
   refresh_forest(ix);
-  if ((rc = buf_reserve(ix->work, sizeof(uint32_t), s, false, 0))) return rc;
+  if ((rc = buf_reserve(ix->qs.work, sizeof(uint32_t), s, false, 0))) return rc;
   BatchDesc b{};
   b.queries = q;
   b.arg = arg;
@@ -311,13 +324,18 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   b.mode = handler;
   b.chunk_begin = 0;
   b.order = nullptr;
+  b.qbase = 0;
+  if (want_sort(ix, n)) {
+    if ((rc = plan_order(ix->qs, &b, 1, n, s))) return rc;
+    if ((rc = fill_order(ix, ix->qs, &b, nullptr, 1, n, s))) return rc;
+  }
   LaunchPlan plan = plan_for(ix, pred);
   uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
   return launch_queries(ix->forest, plan, &b, nullptr, 1, static_cast<uint32_t>(chunks),
-                        static_cast<uint32_t*>(ix->work.ptr), s);
+                        static_cast<uint32_t*>(ix->qs.work.ptr), s);
 }
 
-}  // namespace
+}  // namespace rts
 
 extern "C" {
 
@@ -343,7 +361,8 @@ int rts_config_default(rts_config* c) {
   c->curve = RTS_CURVE_HILBERT;
   c->max_trees = 8;
   c->rebuild_fraction = 0.25f;
-  c->sort_queries = 0;
+  c->sort_queries = 2;
+  c->query_occupancy = 0;
   c->rebuild_update_fraction = 0.25f;
   c->chunk = 0;
   return RTS_OK;
@@ -386,11 +405,13 @@ int rts_destroy(rts_index* ix) {
     buf_free(t.nodes, s);
   }
   DevBuf* all[] = {&ix->leaves, &ix->leaf_ids, &ix->pos, &ix->keys_a, &ix->keys_b, &ix->vals_a,
-                   &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp, &ix->work};
+                   &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp};
   for (DevBuf* b : all) {
     touched |= b->ptr != nullptr;
     buf_free(*b, s);
   }
+  touched |= ix->qs.work.ptr != nullptr;
+  ix->qs.release(s);
   ix->staging.release();
   if (touched) cudaStreamSynchronize(s);  // frees are stream-ordered
   delete ix;
@@ -406,6 +427,7 @@ int rts_clear(rts_index* ix, void* stream) {
   ix->slot_end = 0;
   ix->updated_since_build = 0;
   ix->forest_dirty = true;
+  ix->version++;
   return RTS_OK;
 }
 
@@ -435,6 +457,7 @@ int rts_insert(rts_index* ix, const float* envelopes, uint64_t n, void* stream) 
   ix->n_ids += n;
   ix->slot_end = slot_end;
   ix->forest_dirty = true;
+  ix->version++;
   if (merge) {
     ix->trees.push_back(t);  // no levels yet; rebuild_all only reads its slots
     return rebuild_all(ix, s);
@@ -491,51 +514,29 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   if (n_batches == 0) return RTS_OK;
   if (!batches) return fail(RTS_ERR_INVALID_ARGUMENT, "batches is null");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  std::vector<BatchDesc> descs;
-  descs.reserve(n_batches);
-  uint64_t chunks = 0;
-  int rc;
   LaunchPlan plan = plan_for(ix, kContains);
-  for (uint32_t i = 0; i < n_batches; ++i) {
-    const rts_batch& b = batches[i];
-    if ((rc = check_handler(b.handler, b.arg))) return rc;
-    int pred;
-    if (b.query_kind == RTS_QUERY_POINTS) {
-      if (b.predicate != RTS_PREDICATE_CONTAINS)
-        return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
-      pred = kPoint;
-    } else if (b.query_kind == RTS_QUERY_ENVELOPES) {
-      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
-      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
-      else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
-    } else {
-      return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
-    }
-    if (b.n == 0) continue;
-    if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
-    if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
-    BatchDesc d{};
-    d.queries = b.queries;
-    d.arg = b.arg;
-    d.n = static_cast<uint32_t>(b.n);
-    d.pred = pred;
-    d.mode = b.handler;
-    d.chunk_begin = static_cast<uint32_t>(chunks);
-    d.order = nullptr;
-    chunks += (b.n + plan.chunk - 1) / plan.chunk;
-    if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
-    descs.push_back(d);
-  }
+  std::vector<BatchDesc> descs;
+  uint64_t chunks = 0;
+  int rc = make_descs(ix, batches, n_batches, plan, descs, chunks);
+  if (rc) return rc;
   if (descs.empty() || ix->n_ids == 0) return RTS_OK;
   refresh_forest(ix);
-  if ((rc = buf_reserve(ix->work, sizeof(uint32_t), s, false, 0))) return rc;
+  if ((rc = buf_reserve(ix->qs.work, sizeof(uint32_t), s, false, 0))) return rc;
+  uint64_t total = 0;
+  for (const auto& d : descs) total += d.n;
+  const bool sorted = want_sort(ix, total);
+  if (sorted && (rc = plan_order(ix->qs, descs.data(), static_cast<uint32_t>(descs.size()), total, s)))
+    return rc;
   void* ddev = nullptr;
   if (descs.size() > 1 &&
       (rc = ix->staging.put(descs.data(), descs.size() * sizeof(BatchDesc), s, &ddev)))
     return rc;
+  if (sorted && (rc = fill_order(ix, ix->qs, descs.data(), static_cast<const BatchDesc*>(ddev),
+                                 static_cast<uint32_t>(descs.size()), total, s)))
+    return rc;
   return launch_queries(ix->forest, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
                         static_cast<uint32_t>(descs.size()), static_cast<uint32_t>(chunks),
-                        static_cast<uint32_t*>(ix->work.ptr), s);
+                        static_cast<uint32_t*>(ix->qs.work.ptr), s);
 }
 
 uint64_t rts_size(const rts_index* ix) { return ix ? ix->n_ids : 0; }

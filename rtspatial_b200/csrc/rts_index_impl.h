@@ -1,0 +1,113 @@
+// Internal definition of the index object behind the C-ABI, shared by the
+// index calls (rts_index.cu), prepared launches (rts_plan.cu) and the serving
+// engine (rts_server.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "rts_internal.h"
+
+namespace rts {
+
+// Pinned staging for small host->device copies that must not block the host:
+// a ring of slots, each reused only after the copy that last read it is done.
+struct Staging {
+  static constexpr int kSlots = 4;
+  void* host[kSlots] = {};
+  DevBuf dev[kSlots];
+  size_t host_bytes[kSlots] = {};
+  cudaEvent_t done[kSlots] = {};
+  int next = 0;
+
+  // Copies `bytes` from src to a device buffer; returns its device address.
+  int put(const void* src, size_t bytes, cudaStream_t s, void** dev_out) {
+    int k = next;
+    next = (next + 1) % kSlots;
+    if (done[k]) RTS_CUDA_TRY(cudaEventSynchronize(done[k]));
+    else RTS_CUDA_TRY(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+    if (host_bytes[k] < bytes) {
+      if (host[k]) cudaFreeHost(host[k]);
+      host[k] = nullptr;
+      size_t cap = std::max<size_t>(bytes, 4096);
+      RTS_CUDA_TRY(cudaMallocHost(&host[k], cap));
+      host_bytes[k] = cap;
+    }
+    int rc = buf_reserve(dev[k], bytes, s, false, 0);
+    if (rc) return rc;
+    std::memcpy(host[k], src, bytes);
+    RTS_CUDA_TRY(cudaMemcpyAsync(dev[k].ptr, host[k], bytes, cudaMemcpyHostToDevice, s));
+    RTS_CUDA_TRY(cudaEventRecord(done[k], s));
+    *dev_out = dev[k].ptr;
+    return RTS_OK;
+  }
+  void release() {
+    for (int k = 0; k < kSlots; ++k) {
+      if (done[k]) {
+        cudaEventSynchronize(done[k]);
+        cudaEventDestroy(done[k]);
+        done[k] = nullptr;
+      }
+      if (host[k]) cudaFreeHost(host[k]);
+      host[k] = nullptr;
+      host_bytes[k] = 0;
+      buf_free(dev[k], 0);
+    }
+  }
+};
+
+// Scratch of one query launch in flight: work counter and the buffers of the
+// query visiting-order sort.  Launches that may run concurrently need their
+// own QueryScratch.
+struct QueryScratch {
+  DevBuf work, keys_a, keys_b, vals, order, sort_temp;
+  void release(cudaStream_t s) {
+    buf_free(work, s);
+    buf_free(keys_a, s);
+    buf_free(keys_b, s);
+    buf_free(vals, s);
+    buf_free(order, s);
+    buf_free(sort_temp, s);
+  }
+};
+
+constexpr uint64_t kSlotAlign = 32;
+
+}  // namespace rts
+
+struct rts_index {
+  rts_config cfg{};
+  int W = 8;
+  uint64_t n_ids = 0;
+  uint64_t slot_end = 0;        // slots in use (each sub-tree padded to 32)
+  uint64_t updated_since_build = 0;
+  uint64_t version = 0;         // bumped when buffers or sub-trees change
+  rts::DevBuf leaves, leaf_ids, pos;
+  std::vector<rts::HostTree> trees;
+  // scratch of the build path
+  rts::DevBuf keys_a, keys_b, vals_a, vals_b, sort_temp, bounds, slots_tmp;
+  // scratch of this index's own query calls
+  rts::QueryScratch qs;
+  rts::Staging staging;
+  rts::Forest forest{};
+  bool forest_dirty = true;
+};
+
+namespace rts {
+
+inline uint64_t round_up(uint64_t a, uint64_t b) { return (a + b - 1) / b * b; }
+
+void refresh_forest(rts_index* ix);
+LaunchPlan plan_for(const rts_index* ix, int pred);
+bool want_sort(const rts_index* ix, uint64_t total);
+int check_handler(int handler, void* arg);
+int plan_order(QueryScratch& qs, BatchDesc* descs, uint32_t nd, uint64_t total, cudaStream_t s);
+int fill_order(rts_index* ix, QueryScratch& qs, const BatchDesc* host, const BatchDesc* dev,
+               uint32_t nd, uint64_t total, cudaStream_t s);
+int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
+               const LaunchPlan& plan, std::vector<BatchDesc>& out, uint64_t& chunks);
+
+}  // namespace rts

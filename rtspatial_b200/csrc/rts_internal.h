@@ -71,6 +71,14 @@ int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_
 // {id_begin, n, slot_base} per tree.
 int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint32_t* slots,
                      cudaStream_t s);
+// Visiting order of the queries of nb batches: sorts (batch, curve key of the
+// query centre) and writes each batch's query indices to order[qbase ...].
+int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
+                       const float4* frame_box, int curve, unsigned long long* keys_a,
+                       unsigned long long* keys_b, uint32_t* vals_a, uint32_t* order,
+                       DevBuf& temp, cudaStream_t s);
+// Temporary bytes the order sort of `total` queries in `nb` batches needs.
+int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes);
 int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
                   float4* leaves, cudaStream_t s);
 int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
@@ -81,6 +89,7 @@ struct LaunchPlan {
   int width = 8;
   bool team = false;
   uint32_t chunk = 32;  // queries per work item
+  bool high_occupancy = false;  // cap registers for 4 CTAs of 256 threads per SM
 };
 // Runs `nb` batches (descriptors in host memory `hb`; device copy `db` when
 // nb > 1) in one persistent launch.  work_counter: zeroed device uint32.

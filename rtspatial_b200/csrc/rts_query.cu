@@ -37,8 +37,8 @@ __device__ __noinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B,
 
 constexpr int kQueryThreads = 256;
 
-template <int W, bool TEAM>
-__global__ void __launch_bounds__(kQueryThreads)
+template <int W, bool TEAM, int MINB>
+__global__ void __launch_bounds__(kQueryThreads, MINB)
     k_query(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
             const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
             uint32_t chunk, uint32_t* __restrict__ work) {
@@ -75,23 +75,28 @@ __global__ void __launch_bounds__(kQueryThreads)
 using QueryKernel = void (*)(const Forest, const BatchDesc, const BatchDesc*, uint32_t, uint32_t,
                              uint32_t, uint32_t*);
 
-static QueryKernel pick_kernel(const LaunchPlan& p) {
+template <int MINB>
+static QueryKernel pick_kernel_occ(const LaunchPlan& p) {
   if (p.team) {
     switch (p.width) {
-      case 4: return k_query<4, true>;
-      case 8: return k_query<8, true>;
-      case 16: return k_query<16, true>;
-      case 32: return k_query<32, true>;
+      case 4: return k_query<4, true, MINB>;
+      case 8: return k_query<8, true, MINB>;
+      case 16: return k_query<16, true, MINB>;
+      case 32: return k_query<32, true, MINB>;
     }
   } else {
     switch (p.width) {
-      case 4: return k_query<4, false>;
-      case 8: return k_query<8, false>;
-      case 16: return k_query<16, false>;
-      case 32: return k_query<32, false>;
+      case 4: return k_query<4, false, MINB>;
+      case 8: return k_query<8, false, MINB>;
+      case 16: return k_query<16, false, MINB>;
+      case 32: return k_query<32, false, MINB>;
     }
   }
   return nullptr;
+}
+
+static QueryKernel pick_kernel(const LaunchPlan& p) {
+  return p.high_occupancy ? pick_kernel_occ<4>(p) : pick_kernel_occ<1>(p);
 }
 
 static int g_num_sms = 0;

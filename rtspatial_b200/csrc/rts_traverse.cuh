@@ -28,7 +28,8 @@ struct BatchDesc {
   int32_t mode;           // HandlerKind
   uint32_t chunk_begin;   // index of the batch's first chunk in the launch
   const uint32_t* order;  // optional visiting order (query ids), or nullptr
-  uint32_t pad[2];
+  uint32_t qbase;         // offset of the batch in the launch's concatenated order
+  uint32_t pad;
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {

@@ -76,9 +76,10 @@ class Config:
     curve: int = L.RTS_CURVE_HILBERT
     max_trees: int = 8
     rebuild_fraction: float = 0.25
-    sort_queries: bool = False
+    sort_queries: int = 2
     rebuild_update_fraction: float = 0.25
     chunk: int = 0
+    query_occupancy: int = 0
 
     def to_c(self) -> L.rts_config:
         c = L.rts_config()
@@ -277,20 +278,14 @@ class SpatialIndex:
     def query_batched(self, batches: Sequence[tuple], stream=None) -> None:
         """Runs several Query calls in one persistent launch.  Each batch is
         ``(predicate, queries, handler, arg)``; points are (n, 2) tensors."""
-        arr = (L.rts_batch * len(batches))()
-        keep = []
-        for i, (pred, q, handler, arg) in enumerate(batches):
-            is_pt = q.dim() == 2 and q.shape[1] == 2
-            q = _f32(q, 2 if is_pt else 4, "queries")
-            keep.append(q)
-            arr[i].query_kind = L.RTS_QUERY_POINTS if is_pt else L.RTS_QUERY_ENVELOPES
-            arr[i].predicate = int(pred)
-            arr[i].queries = q.data_ptr()
-            arr[i].n = q.shape[0]
-            arr[i].handler = int(handler)
-            arr[i].arg = arg
+        arr, keep = _batch_array(batches)
         check(lib().rts_query_batched(self._handle(), arr, len(batches), _stream_handle(stream)))
         self._keep = keep
+
+    def plan(self, batches: Sequence[tuple]) -> "Plan":
+        """A prepared launch of fixed batches, replayable through a CUDA graph
+        (``rts_plan_*``).  Query tensors and outputs must stay allocated."""
+        return Plan(self, batches)
 
     # -- introspection ------------------------------------------------------------
     def size(self) -> int:
@@ -304,6 +299,46 @@ class SpatialIndex:
 
     def PrintMemoryUsage(self) -> None:
         print(f"Index {self.memory_usage() / 2**20:.1f} MB")
+
+
+def _batch_array(batches):
+    arr = (L.rts_batch * len(batches))()
+    keep = []
+    for i, (pred, q, handler, arg) in enumerate(batches):
+        is_pt = q.dim() == 2 and q.shape[1] == 2
+        q = _f32(q, 2 if is_pt else 4, "queries")
+        keep.append(q)
+        arr[i].query_kind = L.RTS_QUERY_POINTS if is_pt else L.RTS_QUERY_ENVELOPES
+        arr[i].predicate = int(pred)
+        arr[i].queries = q.data_ptr()
+        arr[i].n = q.shape[0]
+        arr[i].handler = int(handler)
+        arr[i].arg = arg
+    return arr, keep
+
+
+class Plan:
+    """Prepared batched launch (``rts_plan_create/launch/destroy``)."""
+
+    def __init__(self, index: "SpatialIndex", batches: Sequence[tuple]):
+        self.index = index
+        arr, self._keep = _batch_array(batches)
+        self._h = ctypes.c_void_p()
+        check(lib().rts_plan_create(index._handle(), arr, len(batches), ctypes.byref(self._h)))
+
+    def launch(self, stream=None, graph: bool = True) -> None:
+        check(lib().rts_plan_launch(self._h, _stream_handle(stream), 1 if graph else 0))
+
+    def close(self) -> None:
+        if self._h:
+            lib().rts_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def sort_pairs(p: torch.Tensor) -> torch.Tensor:

@@ -12,8 +12,8 @@ EXE = os.path.join(HERE, "cpp", "_build", "test_spatial_index")
 
 
 def test_cpp_dropin_api(cuda):
-    if not os.path.exists(EXE):
-        subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "cpp")])
+    # always re-make: a binary built against an older header must not run
+    subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "cpp")])
     r = subprocess.run([EXE], capture_output=True, text=True, timeout=600)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr

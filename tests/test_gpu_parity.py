@@ -76,9 +76,10 @@ def workloads(oracle):
 
 @pytest.mark.parametrize("combo", SOME_COMBOS, ids=combo_id)
 @pytest.mark.parametrize("name", ["uniform", "clustered", "lognormal"])
-def test_random_parity(cuda, workloads, combo, name):
+@pytest.mark.parametrize("order", [0, 1], ids=["as-given", "curve-sorted"])
+def test_random_parity(cuda, workloads, combo, name, order):
     b, p, q, want = workloads[name]
-    ix = make_index(combo)
+    ix = make_index(combo, sort_queries=order)
     ix.Insert(dev(b))
     assert_same_pairs(gpu_pairs(ix, P.kContains, p), want["point"], f"{name} point")
     assert_same_pairs(gpu_pairs(ix, P.kContains, q), want["contains"], f"{name} contains")
@@ -132,9 +133,11 @@ def test_queue_overflow_reports_needed_size(cuda, oracle):
 
 
 @pytest.mark.parametrize("combo", SOME_COMBOS, ids=combo_id)
-def test_batched_equals_plain(cuda, workloads, combo):
+@pytest.mark.parametrize("order", [0, 1], ids=["as-given", "curve-sorted"])
+@pytest.mark.parametrize("occ", [0, 4], ids=["occ-default", "occ-4"])
+def test_batched_equals_plain(cuda, workloads, combo, order, occ):
     b, p, q, want = workloads["clustered"]
-    ix = make_index(combo)
+    ix = make_index(combo, sort_queries=order, query_occupancy=occ)
     ix.Insert(dev(b))
     rng = np.random.default_rng(1)
     specs = []
