@@ -39,6 +39,7 @@ extern "C" {
 #define RTS_ERR_QUEUE_FULL 4   /* a collecting queue received more pairs than its capacity */
 #define RTS_ERR_CAPACITY 5     /* a size exceeds a documented maximum */
 #define RTS_ERR_UNSUPPORTED 6
+#define RTS_ERR_TIMEOUT 7      /* a wait ended before the request was done */
 
 /* ---- predicates: values of rtspatial::Predicate (geom/predicates.h:7-10) - */
 #define RTS_PREDICATE_INTERSECTS 0
@@ -200,6 +201,84 @@ int rts_plan_create(rts_index* index, const rts_batch* batches, uint32_t n_batch
                     rts_plan** out);
 int rts_plan_launch(rts_plan* plan, void* stream, int use_graph);
 int rts_plan_destroy(rts_plan* plan);
+
+/* Refit-vs-rebuild tuner (no counterpart in the reference, which always
+ * refits the touched GASes, spatial_index.cuh:237-264).  Report the duration
+ * of the query work that runs between updates (e.g. one round); the library
+ * models it as t0 * (1 + a * f), f = fraction of boxes updated since the last
+ * re-sort, times its own re-sorts (R), and sets rebuild_update_fraction to
+ * sqrt(2 R u / (t0 a)) (u = updated fraction per report), the value that
+ * minimises re-sort cost plus expected query slowdown.  The new threshold is
+ * returned in *rebuild_update_fraction (nullable). */
+int rts_report_query_time(rts_index* index, double query_ms, float* rebuild_update_fraction);
+
+/* ---- autotuner ----------------------------------------------------------------
+ * No counterpart in the reference (its only tuning is the intersects
+ * parallelism cost model, spatial_index.cuh:690-760, which does not exist
+ * here).  Times candidate launch settings — traversal scheme, register cap,
+ * curve-ordered visiting, chunk size and, with tune_width, the node width
+ * (= leaf size) — on the given batches and keeps the fastest in the index.
+ * The batches run through the tuner's own counters and queues: their handlers
+ * and outputs are not touched.  With tune_width the index is re-sorted at
+ * each candidate width and left at the fastest (its sub-trees merge into
+ * one).  Synchronous. */
+typedef struct rts_tune_result {
+  int32_t node_width, traversal, query_occupancy, sort_queries;
+  uint32_t chunk, candidates;
+  int32_t collecting; /* 1: timed with the collecting handler, 0: counting (huge results) */
+  int32_t reserved;
+  double best_ms;     /* median launch time of the kept settings */
+  double first_ms;    /* median launch time of the first candidate */
+} rts_tune_result;
+int rts_autotune(rts_index* index, const rts_batch* batches, uint32_t n_batches, int tune_width,
+                 void* stream, rts_tune_result* out);
+
+/* ---- serving engine ---------------------------------------------------------
+ * No counterpart in the reference (its Query is a blocking-free launch per
+ * call with no admission or batching).  A server owns an index while it
+ * exists and serves requests from any host thread in submission order:
+ * query requests (host arrays of any size) are cut into parts and packed
+ * into persistent launches, several launches in flight on their own streams;
+ * a part is admitted while its launch's device arena has room for its queries
+ * and estimated pairs.  Update requests (deletes, inserts, updates) apply
+ * after every query submitted before them and before every later one.  A
+ * request's pairs carry its own 0-based query ids and equal those of the same
+ * query made alone on the index state it was submitted against. */
+typedef struct rts_server rts_server;
+typedef struct rts_server_config {
+  uint32_t slots;                  /* launches in flight (1..8) */
+  uint32_t max_parts_per_launch;   /* request parts per launch */
+  uint64_t max_queries_per_launch; /* query capacity of one launch arena */
+  uint64_t pairs_per_launch;       /* pair capacity of one launch arena */
+  uint64_t hbm_budget_bytes;       /* bound on all arenas (0 = half the free HBM) */
+} rts_server_config;
+typedef struct rts_server_stats {
+  uint64_t requests_done, queries_done, pairs_done, launches, retried_parts, updates_done;
+  double latency_p50_s, latency_p99_s, latency_max_s; /* submit -> results on the host */
+  double elapsed_s;                                   /* first submit -> last completion */
+} rts_server_stats;
+int rts_server_config_default(rts_server_config* cfg);
+int rts_server_create(rts_index* index, const rts_server_config* cfg, rts_server** out);
+/* Finishes every submitted request, then stops. */
+int rts_server_destroy(rts_server* server);
+/* Copies the n queries (points: 2 floats, envelopes: 4) and returns a ticket. */
+int rts_server_submit_query(rts_server* server, int query_kind, int predicate,
+                            const float* queries, uint64_t n, uint64_t* ticket);
+/* Copies an update batch: deletes, then updates, then inserts (new ids are
+ * handed out in submission order; rts_server_take reports the first one). */
+int rts_server_submit_update(rts_server* server, const uint64_t* delete_ids, uint64_t n_delete,
+                             const float* insert_envelopes, uint64_t n_insert,
+                             const rts_update_entry* updates, uint64_t n_update,
+                             uint64_t* ticket);
+/* Waits until the request is done (timeout < 0: no limit); RTS_ERR_TIMEOUT. */
+int rts_server_wait(rts_server* server, uint64_t ticket, double timeout_s);
+/* Copies a done query's pairs (RTS_ERR_QUEUE_FULL with *n_pairs set when
+ * capacity is too small) and forgets the ticket.  For an update ticket,
+ * *n_pairs = the first id its inserts received. */
+int rts_server_take(rts_server* server, uint64_t ticket, rts_pair* out, uint64_t capacity,
+                    uint64_t* n_pairs);
+int rts_server_get_stats(rts_server* server, rts_server_stats* stats);
+int rts_server_reset_stats(rts_server* server);
 
 /* No counterpart in the reference.  The same as rts_query_batched, but it
  * allocates no memory: for callers that cannot call cudaMalloc once they are

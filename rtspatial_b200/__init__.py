@@ -18,6 +18,7 @@ from .spatial_index import (  # noqa: F401
     SpatialIndex,
     sort_pairs,
 )
+from .server import Server  # noqa: F401
 
 __all__ = ["Config", "Counter", "Handler", "Plan", "Predicate", "Queue", "SpatialIndex", "sort_pairs",
-           "RtsError", "lib", "LIB_PATH"]
+           "RtsError", "lib", "LIB_PATH", "Server"]

@@ -19,6 +19,7 @@ RTS_ERR_OUT_OF_MEMORY = 3
 RTS_ERR_QUEUE_FULL = 4
 RTS_ERR_CAPACITY = 5
 RTS_ERR_UNSUPPORTED = 6
+RTS_ERR_TIMEOUT = 7
 
 RTS_PREDICATE_INTERSECTS = 0
 RTS_PREDICATE_CONTAINS = 1
@@ -82,6 +83,28 @@ class rts_batch(ctypes.Structure):
     ]
 
 
+class rts_server_config(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("max_parts_per_launch", ctypes.c_uint32),
+                ("max_queries_per_launch", ctypes.c_uint64), ("pairs_per_launch", ctypes.c_uint64),
+                ("hbm_budget_bytes", ctypes.c_uint64)]
+
+
+class rts_server_stats(ctypes.Structure):
+    _fields_ = [("requests_done", ctypes.c_uint64), ("queries_done", ctypes.c_uint64),
+                ("pairs_done", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("retried_parts", ctypes.c_uint64), ("updates_done", ctypes.c_uint64),
+                ("latency_p50_s", ctypes.c_double), ("latency_p99_s", ctypes.c_double),
+                ("latency_max_s", ctypes.c_double), ("elapsed_s", ctypes.c_double)]
+
+
+class rts_tune_result(ctypes.Structure):
+    _fields_ = [("node_width", ctypes.c_int32), ("traversal", ctypes.c_int32),
+                ("query_occupancy", ctypes.c_int32), ("sort_queries", ctypes.c_int32),
+                ("chunk", ctypes.c_uint32), ("candidates", ctypes.c_uint32),
+                ("collecting", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("best_ms", ctypes.c_double), ("first_ms", ctypes.c_double)]
+
+
 # name -> (restype, argtypes); every symbol the header declares.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -101,6 +124,18 @@ SIGNATURES = {
     "rts_plan_create": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, ctypes.POINTER(_P)]),
     "rts_plan_launch": (_I, [_P, _P, _I]),
     "rts_plan_destroy": (_I, [_P]),
+    "rts_server_config_default": (_I, [ctypes.POINTER(rts_server_config)]),
+    "rts_server_create": (_I, [_P, ctypes.POINTER(rts_server_config), ctypes.POINTER(_P)]),
+    "rts_server_destroy": (_I, [_P]),
+    "rts_server_submit_query": (_I, [_P, _I, _I, _P, _U64, ctypes.POINTER(_U64)]),
+    "rts_server_submit_update": (_I, [_P, _P, _U64, _P, _U64, _P, _U64, ctypes.POINTER(_U64)]),
+    "rts_server_wait": (_I, [_P, _U64, ctypes.c_double]),
+    "rts_server_take": (_I, [_P, _U64, _P, _U64, ctypes.POINTER(_U64)]),
+    "rts_server_get_stats": (_I, [_P, ctypes.POINTER(rts_server_stats)]),
+    "rts_server_reset_stats": (_I, [_P]),
+    "rts_autotune": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _I, _P,
+                          ctypes.POINTER(rts_tune_result)]),
+    "rts_report_query_time": (_I, [_P, ctypes.c_double, ctypes.POINTER(ctypes.c_float)]),
     "rts_size": (_U64, [_P]),
     "rts_num_trees": (ctypes.c_uint32, [_P]),
     "rts_memory_usage": (_U64, [_P]),

@@ -284,6 +284,78 @@ __device__ __forceinline__ void collect_warp(const DevQueue& qu, uint32_t m,
   }
 }
 
+// Warp-private staging of collected pairs in shared memory.  Pairs found in a
+// step are written to the warp's buffer; the buffer is flushed to the queue
+// with one atomicAdd and coalesced 8-byte stores when it would overflow and
+// when the warp finishes its chunk.  All calls are made by all 32 lanes.
+constexpr uint32_t kWarpOutCap = 256;
+
+struct WarpOut {
+  DevPair* buf;   // kWarpOutCap entries in shared memory, private to the warp
+  uint32_t n;     // pairs buffered (same value in every lane)
+
+  __device__ __forceinline__ void flush(const DevQueue& qu) {
+    if (n == 0) return;
+    __syncwarp();
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(qu.size, n);
+    base = __shfl_sync(kFull, base, 0);
+    for (uint32_t i = lane_id(); i < n; i += 32) {
+      unsigned long long p = static_cast<unsigned long long>(base) + i;
+      if (p < qu.capacity) qu.data[p] = buf[i];
+    }
+    __syncwarp();
+    n = 0;
+  }
+
+  // Adds, for every lane, (ids[c], qid) for each set bit c of m.
+  __device__ __forceinline__ void add(const DevQueue& qu, uint32_t m, const uint32_t* ids,
+                                      uint32_t qid) {
+    if (!__any_sync(kFull, m != 0)) return;
+    const uint32_t lane = lane_id();
+    uint32_t cnt = __popc(m);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(kFull, incl, o);
+      if (lane >= static_cast<uint32_t>(o)) incl += v;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (n + total > kWarpOutCap) flush(qu);
+    if (total > kWarpOutCap) {  // more than a buffer: straight to the queue
+      uint32_t base = 0;
+      if (lane == 31) base = atomicAdd(qu.size, total);
+      base = __shfl_sync(kFull, base, 31);
+      unsigned long long p = static_cast<unsigned long long>(base) + (incl - cnt);
+      while (m) {
+        int c = __ffs(m) - 1;
+        m &= m - 1;
+        if (p < qu.capacity) qu.data[p] = DevPair{ids[c], qid};
+        ++p;
+      }
+      return;
+    }
+    uint32_t at = n + incl - cnt;
+    while (m) {
+      int c = __ffs(m) - 1;
+      m &= m - 1;
+      buf[at++] = DevPair{ids[c], qid};
+    }
+    n += total;
+  }
+
+  // Team scheme: each lane has at most one pair.
+  __device__ __forceinline__ void add_one(const DevQueue& qu, bool hit, uint32_t gid,
+                                          uint32_t qid) {
+    const uint32_t bal = __ballot_sync(kFull, hit);
+    if (bal == 0) return;
+    const uint32_t total = __popc(bal);
+    if (n + total > kWarpOutCap) flush(qu);
+    if (hit) buf[n + __popc(bal & ((1u << lane_id()) - 1u))] = DevPair{gid, qid};
+    n += total;
+  }
+};
+
 // Lane-count reduction for the counting handler, one atomic per warp.
 __device__ __forceinline__ void count_flush_warp(unsigned long long* counter,
                                                  unsigned long long v) {

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -133,11 +134,30 @@ int sort_into_slots(rts_index* ix, const float4* src, const uint32_t* src_ids, c
   return launch_fill_pad(dst_leaves, dst_ids, slot_base + n, slot_base + round_up(n, kSlotAlign), s);
 }
 
+int rebuild_all_impl(rts_index* ix, cudaStream_t s);
+
 // Re-sorts every box of the index into one tree.
 int rebuild_all(rts_index* ix, cudaStream_t s) {
   const uint64_t N = ix->n_ids;
   int rc;
   if (N == 0) return RTS_OK;
+  if (!ix->ev_rebuild0) {
+    RTS_CUDA_TRY(cudaEventCreate(&ix->ev_rebuild0));
+    RTS_CUDA_TRY(cudaEventCreate(&ix->ev_rebuild1));
+  }
+  RTS_CUDA_TRY(cudaEventRecord(ix->ev_rebuild0, s));
+  rc = rebuild_all_impl(ix, s);
+  if (rc) return rc;
+  RTS_CUDA_TRY(cudaEventRecord(ix->ev_rebuild1, s));
+  ix->rebuild_timed = true;
+  ix->t0_ms = 0;
+  ix->updated_at_report = 0;
+  return RTS_OK;
+}
+
+int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
+  const uint64_t N = ix->n_ids;
+  int rc;
   // slots_tmp[k] = slot of the k-th id-ordered entry, tree by tree.
   std::vector<uint64_t> meta;
   uint64_t max_n = 0;
@@ -410,6 +430,8 @@ int rts_destroy(rts_index* ix) {
     touched |= b->ptr != nullptr;
     buf_free(*b, s);
   }
+  if (ix->ev_rebuild0) cudaEventDestroy(ix->ev_rebuild0);
+  if (ix->ev_rebuild1) cudaEventDestroy(ix->ev_rebuild1);
   touched |= ix->qs.work.ptr != nullptr;
   ix->qs.release(s);
   ix->staging.release();
@@ -537,6 +559,39 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   return launch_queries(ix->forest, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
                         static_cast<uint32_t>(descs.size()), static_cast<uint32_t>(chunks),
                         static_cast<uint32_t*>(ix->qs.work.ptr), s);
+}
+
+int rts_report_query_time(rts_index* ix, double query_ms, float* rebuild_update_fraction) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (!(query_ms > 0)) return fail(RTS_ERR_INVALID_ARGUMENT, "query time must be positive");
+  if (ix->rebuild_timed) {
+    float ms = 0;
+    if (cudaEventQuery(ix->ev_rebuild1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, ix->ev_rebuild0, ix->ev_rebuild1) == cudaSuccess) {
+      ix->rebuild_ms = ms;
+      ix->rebuild_timed = false;
+    }
+  }
+  const double n = static_cast<double>(std::max<uint64_t>(ix->n_ids, 1));
+  const double f = static_cast<double>(ix->updated_since_build) / n;
+  const double df = static_cast<double>(ix->updated_since_build - ix->updated_at_report) / n;
+  ix->updated_at_report = ix->updated_since_build;
+  if (ix->t0_ms <= 0 || f == 0) {
+    ix->t0_ms = (ix->t0_ms <= 0) ? query_ms : std::min(ix->t0_ms, query_ms);
+  } else {
+    if (df > 0) ix->upd_per_report = (ix->upd_per_report > 0) ? 0.7 * ix->upd_per_report + 0.3 * df : df;
+    const double a = std::max(0.0, (query_ms / ix->t0_ms - 1.0) / f);
+    ix->slope = (ix->slope > 0) ? 0.7 * ix->slope + 0.3 * a : a;
+  }
+  // Cost per report of re-sorting every F of updates: R * u / F; expected
+  // extra query time per report: t0 * a * F / 2.  Minimum at
+  // F* = sqrt(2 R u / (t0 a)).
+  if (ix->rebuild_ms > 0 && ix->slope > 0 && ix->upd_per_report > 0 && ix->t0_ms > 0) {
+    double F = std::sqrt(2.0 * ix->rebuild_ms * ix->upd_per_report / (ix->t0_ms * ix->slope));
+    ix->cfg.rebuild_update_fraction = static_cast<float>(std::min(1.0, std::max(0.005, F)));
+  }
+  if (rebuild_update_fraction) *rebuild_update_fraction = ix->cfg.rebuild_update_fraction;
+  return RTS_OK;
 }
 
 uint64_t rts_size(const rts_index* ix) { return ix ? ix->n_ids : 0; }

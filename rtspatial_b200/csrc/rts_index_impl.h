@@ -94,6 +94,14 @@ struct rts_index {
   rts::Staging staging;
   rts::Forest forest{};
   bool forest_dirty = true;
+  // refit-vs-rebuild tuner state
+  cudaEvent_t ev_rebuild0 = nullptr, ev_rebuild1 = nullptr;
+  bool rebuild_timed = false;       // events recorded around the last re-sort
+  double rebuild_ms = 0;            // duration of the last re-sort
+  double t0_ms = 0;                 // query time reported right after a re-sort
+  uint64_t updated_at_report = 0;   // updated_since_build at the previous report
+  double upd_per_report = 0;        // EMA of the updated fraction between reports
+  double slope = 0;                 // EMA of a in t = t0 * (1 + a * f)
 };
 
 namespace rts {
@@ -101,6 +109,8 @@ namespace rts {
 inline uint64_t round_up(uint64_t a, uint64_t b) { return (a + b - 1) / b * b; }
 
 void refresh_forest(rts_index* ix);
+// Re-sorts every box of the index into one tree at the index's node width.
+int rebuild_all(rts_index* ix, cudaStream_t s);
 LaunchPlan plan_for(const rts_index* ix, int pred);
 bool want_sort(const rts_index* ix, uint64_t total);
 int check_handler(int handler, void* arg);

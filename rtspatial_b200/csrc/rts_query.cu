@@ -13,24 +13,30 @@ namespace rts {
 
 template <int W, bool TEAM, int PRED, int MODE>
 __device__ __forceinline__ void run_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                          uint32_t ce) {
+                                          uint32_t ce, DevPair* wbuf) {
   if constexpr (TEAM) {
-    run_chunk_team<PRED, MODE, W>(F, B, cb, ce);
+    run_chunk_team<PRED, MODE, W>(F, B, cb, ce, wbuf);
   } else {
-    run_chunk_thread<PRED, MODE, W>(F, B, cb, ce);
+    run_chunk_thread<PRED, MODE, W>(F, B, cb, ce, wbuf);
   }
 }
 
 template <int W, bool TEAM>
 __device__ __noinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                            uint32_t ce) {
+                                            uint32_t ce, DevPair* wbuf) {
   switch (B.pred * 2 + B.mode) {
-    case kPoint * 2 + kCount: run_chunk<W, TEAM, kPoint, kCount>(F, B, cb, ce); break;
-    case kPoint * 2 + kCollect: run_chunk<W, TEAM, kPoint, kCollect>(F, B, cb, ce); break;
-    case kContains * 2 + kCount: run_chunk<W, TEAM, kContains, kCount>(F, B, cb, ce); break;
-    case kContains * 2 + kCollect: run_chunk<W, TEAM, kContains, kCollect>(F, B, cb, ce); break;
-    case kIntersects * 2 + kCount: run_chunk<W, TEAM, kIntersects, kCount>(F, B, cb, ce); break;
-    case kIntersects * 2 + kCollect: run_chunk<W, TEAM, kIntersects, kCollect>(F, B, cb, ce); break;
+    case kPoint * 2 + kCount: run_chunk<W, TEAM, kPoint, kCount>(F, B, cb, ce, wbuf); break;
+    case kPoint * 2 + kCollect: run_chunk<W, TEAM, kPoint, kCollect>(F, B, cb, ce, wbuf); break;
+    case kContains * 2 + kCount: run_chunk<W, TEAM, kContains, kCount>(F, B, cb, ce, wbuf); break;
+    case kContains * 2 + kCollect:
+      run_chunk<W, TEAM, kContains, kCollect>(F, B, cb, ce, wbuf);
+      break;
+    case kIntersects * 2 + kCount:
+      run_chunk<W, TEAM, kIntersects, kCount>(F, B, cb, ce, wbuf);
+      break;
+    case kIntersects * 2 + kCollect:
+      run_chunk<W, TEAM, kIntersects, kCollect>(F, B, cb, ce, wbuf);
+      break;
     default: break;
   }
 }
@@ -43,6 +49,7 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
             const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
             uint32_t chunk, uint32_t* __restrict__ work) {
   __shared__ Forest F;
+  __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&F_in);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&F);
@@ -68,7 +75,7 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     }
     const uint32_t cb = (c - B.chunk_begin) * chunk;
     const uint32_t ce = min(cb + chunk, B.n);
-    dispatch_chunk<W, TEAM>(F, B, cb, ce);
+    dispatch_chunk<W, TEAM>(F, B, cb, ce, wbufs[threadIdx.x / 32]);
   }
 }
 

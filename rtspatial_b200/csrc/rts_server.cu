@@ -1,0 +1,667 @@
+// Serving engine: continuous batching over a resident index.
+//
+// Requests (query batches of any size, and update batches of deletes /
+// inserts / updates) are submitted from any host thread and served in
+// submission order by one worker thread:
+//  - Query requests are cut into parts and packed into launches.  Each launch
+//    runs on one of `slots` streams with its own device arena (query buffer,
+//    pair buffer, per-part queues and counters, sort scratch); a part is
+//    admitted only while the launch's arena has room for its queries and for
+//    its estimated pairs (admission by memory headroom).  While one launch
+//    runs, the next is packed and launched on another slot, and finished
+//    launches copy their pairs back, so requests that arrive while others are
+//    on the GPU are admitted as soon as a slot frees.
+//  - A part whose pairs exceed its estimate is re-run alone with the exact
+//    capacity its counter reported (no pair is lost or duplicated).
+//  - An update request is applied on the update stream after every launch
+//    issued before it and before every launch issued after it (stream
+//    events), so each query sees exactly the updates submitted before it.
+// Each part is one batch of the persistent query kernel with its own 0-based
+// query ids, so a request's pairs are the same whether it ran alone or in a
+// mix; the engine shifts ids by the part's offset in its request.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "rts_index_impl.h"
+
+namespace rts {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_s() {
+  return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+  uint64_t ticket = 0;
+  bool is_update = false;
+  int pred = kPoint;
+  uint32_t qwidth = 2;          // floats per query
+  std::vector<float> q;         // queries (host copy)
+  uint64_t n = 0;               // queries
+  uint64_t next = 0;            // first query not yet admitted
+  uint64_t parts_open = 0;      // admitted parts whose pairs are not back yet
+  std::vector<rts_pair> out;
+  std::vector<uint64_t> del;
+  std::vector<float> ins;
+  std::vector<rts_update_entry> upd;
+  uint64_t first_new_id = 0;
+  int status = RTS_OK;
+  bool done = false;
+  double t_submit = 0, t_done = 0;
+};
+
+struct Part {
+  Request* r = nullptr;
+  uint64_t q0 = 0, nq = 0;      // query range of the request
+  uint64_t in_off = 0;          // byte offset in the slot's query buffer
+  uint64_t out_off = 0;         // pair offset in the slot's pair buffer
+  uint64_t cap = 0;             // pairs reserved
+  uint32_t count = 0;           // pairs reported
+};
+
+struct Retry {
+  Request* r;
+  uint64_t q0, nq, cap;
+};
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  DevBuf d_in, d_pairs, d_counts, d_queues, d_descs;
+  unsigned char* h_in = nullptr;
+  rts_pair* h_pairs = nullptr;
+  uint32_t* h_counts = nullptr;
+  DevQueue* h_queues = nullptr;
+  BatchDesc* h_descs = nullptr;
+  uint64_t in_cap = 0, pair_cap = 0;
+  uint32_t max_parts = 0;
+  QueryScratch qs;
+  cudaEvent_t ev_counts = nullptr, ev_pairs = nullptr, ev_kernel = nullptr;
+  std::vector<Part> parts;
+  int state = 0;  // 0 free, 1 launched, 2 copying pairs
+  bool waited_update = true;
+};
+
+}  // namespace
+}  // namespace rts
+
+using namespace rts;
+
+struct rts_server {
+  rts_index* ix = nullptr;
+  rts_server_config cfg{};
+  int device = 0;
+  std::vector<std::unique_ptr<Slot>> slots;
+  cudaStream_t update_stream = nullptr;
+  cudaEvent_t ev_update = nullptr;
+  bool update_pending_event = false;  // ev_update recorded; slots must wait on it once
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request*> pending;
+  std::deque<Retry> retries;
+  std::deque<Request*> updates_in_flight;
+  std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  std::thread worker;
+  double rate[3] = {4.0, 4.0, 4.0};  // pairs per query estimate per predicate
+  // statistics
+  std::vector<double> lat;
+  uint64_t queries_done = 0, pairs_done = 0, launches = 0, retried = 0, updates_done = 0;
+  double t_first = 0, t_last = 0;
+  int fatal = RTS_OK;
+};
+
+namespace rts {
+namespace {
+
+uint64_t qbytes(const Request* r) { return r->qwidth * sizeof(float); }
+
+int slot_init(rts_server* sv, Slot& sl, uint64_t in_bytes, uint64_t pairs, uint32_t max_parts) {
+  RTS_CUDA_TRY(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+  cudaStream_t s = sl.stream;
+  int rc;
+  if ((rc = buf_reserve(sl.d_in, in_bytes, s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.d_pairs, pairs * sizeof(rts_pair), s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.d_counts, max_parts * sizeof(uint32_t), s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.d_queues, max_parts * sizeof(DevQueue), s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.d_descs, max_parts * sizeof(BatchDesc), s, false, 0))) return rc;
+  RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_in), in_bytes));
+  RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_pairs), pairs * sizeof(rts_pair)));
+  RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_counts), max_parts * sizeof(uint32_t)));
+  RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_queues), max_parts * sizeof(DevQueue)));
+  RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_descs), max_parts * sizeof(BatchDesc)));
+  RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_counts, cudaEventDisableTiming));
+  RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_pairs, cudaEventDisableTiming));
+  RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_kernel, cudaEventDisableTiming));
+  if ((rc = buf_reserve(sl.qs.work, sizeof(uint32_t), s, false, 0))) return rc;
+  // Order scratch for a full slot (so no launch allocates).
+  const uint64_t maxq = in_bytes / (2 * sizeof(float));
+  if ((rc = buf_reserve(sl.qs.keys_a, maxq * 8, s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.qs.keys_b, maxq * 8, s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.qs.vals, maxq * 4, s, false, 0))) return rc;
+  if ((rc = buf_reserve(sl.qs.order, maxq * 4, s, false, 0))) return rc;
+  size_t tb = 0;
+  if ((rc = query_order_temp_bytes(maxq, max_parts, &tb))) return rc;
+  if ((rc = buf_reserve(sl.qs.sort_temp, tb, s, false, 0))) return rc;
+  RTS_CUDA_TRY(cudaStreamSynchronize(s));
+  sl.in_cap = in_bytes;
+  sl.pair_cap = pairs;
+  sl.max_parts = max_parts;
+  (void)sv;
+  return RTS_OK;
+}
+
+void slot_free(Slot& sl) {
+  if (sl.stream) cudaStreamSynchronize(sl.stream);
+  cudaStream_t s = sl.stream;
+  buf_free(sl.d_in, s);
+  buf_free(sl.d_pairs, s);
+  buf_free(sl.d_counts, s);
+  buf_free(sl.d_queues, s);
+  buf_free(sl.d_descs, s);
+  sl.qs.release(s);
+  if (s) cudaStreamSynchronize(s);
+  if (sl.h_in) cudaFreeHost(sl.h_in);
+  if (sl.h_pairs) cudaFreeHost(sl.h_pairs);
+  if (sl.h_counts) cudaFreeHost(sl.h_counts);
+  if (sl.h_queues) cudaFreeHost(sl.h_queues);
+  if (sl.h_descs) cudaFreeHost(sl.h_descs);
+  if (sl.ev_counts) cudaEventDestroy(sl.ev_counts);
+  if (sl.ev_pairs) cudaEventDestroy(sl.ev_pairs);
+  if (sl.ev_kernel) cudaEventDestroy(sl.ev_kernel);
+  if (s) cudaStreamDestroy(s);
+}
+
+void finish_request(rts_server* sv, Request* r) {
+  r->done = true;
+  r->t_done = now_s();
+  sv->t_last = r->t_done;
+  if (!r->is_update) {
+    sv->lat.push_back(r->t_done - r->t_submit);
+    sv->queries_done += r->n;
+  }
+  sv->cv_done.notify_all();
+}
+
+// Packs parts into a free slot and launches them.  Returns true if launched.
+bool admit_and_launch(rts_server* sv, Slot& sl) {
+  rts_index* ix = sv->ix;
+  sl.parts.clear();
+  uint64_t in_used = 0, pair_used = 0;
+  auto add_part = [&](Request* r, uint64_t q0, uint64_t nq, uint64_t cap) {
+    Part p;
+    p.r = r;
+    p.q0 = q0;
+    p.nq = nq;
+    p.in_off = in_used;
+    p.out_off = pair_used;
+    p.cap = cap;
+    in_used += (nq * qbytes(r) + 15) & ~uint64_t(15);
+    pair_used += cap;
+    r->parts_open++;
+    sl.parts.push_back(p);
+  };
+  // Overflowed parts first, each with its exact capacity.
+  while (!sv->retries.empty() && sl.parts.size() < sl.max_parts) {
+    Retry& t = sv->retries.front();
+    uint64_t need_in = (t.nq * qbytes(t.r) + 15) & ~uint64_t(15);
+    if (in_used + need_in > sl.in_cap || pair_used + t.cap > sl.pair_cap) {
+      if (!sl.parts.empty()) break;
+      if (t.cap > sl.pair_cap || need_in > sl.in_cap) {
+        // Cannot fit even alone: split the query range.
+        if (t.nq > 1) {
+          Retry a{t.r, t.q0, t.nq / 2, 0}, b{t.r, t.q0 + t.nq / 2, t.nq - t.nq / 2, 0};
+          a.cap = std::min<uint64_t>(sl.pair_cap, t.cap);
+          b.cap = std::min<uint64_t>(sl.pair_cap, t.cap);
+          sv->retries.pop_front();
+          sv->retries.push_front(b);
+          sv->retries.push_front(a);
+          continue;
+        }
+        t.r->status = RTS_ERR_CAPACITY;  // one query with more pairs than a slot holds
+        sv->retries.pop_front();
+        if (t.r->parts_open == 0 && t.r->next == t.r->n) finish_request(sv, t.r);
+        continue;
+      }
+    }
+    add_part(t.r, t.q0, t.nq, t.cap);
+    sv->retries.pop_front();
+  }
+  // Then requests in submission order, up to the next update.
+  while (!sv->pending.empty() && sl.parts.size() < sl.max_parts) {
+    Request* r = sv->pending.front();
+    if (r->is_update) break;
+    uint64_t room_q = (sl.in_cap - in_used) / qbytes(r);
+    if (room_q == 0) break;
+    uint64_t take = std::min<uint64_t>(r->n - r->next, room_q);
+    double rate = sv->rate[r->pred];
+    uint64_t room_p = sl.pair_cap - pair_used;
+    uint64_t est = static_cast<uint64_t>(static_cast<double>(take) * rate * 1.5) + 64;
+    if (est > room_p) {
+      // shrink the part to what the pair room supports
+      uint64_t t2 = static_cast<uint64_t>(static_cast<double>(room_p > 64 ? room_p - 64 : 0) /
+                                          std::max(rate * 1.5, 1e-9));
+      if (t2 == 0 && !sl.parts.empty()) break;
+      take = std::max<uint64_t>(1, std::min(take, t2));
+      est = std::min<uint64_t>(room_p, static_cast<uint64_t>(take * rate * 1.5) + 64);
+      if (est == 0) break;
+    }
+    add_part(r, r->next, take, est);
+    r->next += take;
+    if (r->next == r->n) sv->pending.pop_front();
+  }
+  if (sl.parts.empty()) return false;
+
+  cudaStream_t s = sl.stream;
+  if (sv->update_pending_event && !sl.waited_update) {
+    cudaStreamWaitEvent(s, sv->ev_update, 0);
+    sl.waited_update = true;
+  }
+  const uint32_t np = static_cast<uint32_t>(sl.parts.size());
+  auto* d_in = static_cast<unsigned char*>(sl.d_in.ptr);
+  auto* d_pairs = static_cast<DevPair*>(sl.d_pairs.ptr);
+  auto* d_counts = static_cast<uint32_t*>(sl.d_counts.ptr);
+  auto* d_queues = static_cast<DevQueue*>(sl.d_queues.ptr);
+  LaunchPlan plan = plan_for(ix, kContains);
+  uint64_t chunks = 0, total = 0;
+  for (uint32_t i = 0; i < np; ++i) {
+    const Part& p = sl.parts[i];
+    std::memcpy(sl.h_in + p.in_off, p.r->q.data() + p.q0 * p.r->qwidth, p.nq * qbytes(p.r));
+    sl.h_queues[i] = DevQueue{d_pairs + p.out_off, p.cap, d_counts + i};
+    BatchDesc d{};
+    d.queries = reinterpret_cast<const float*>(d_in + p.in_off);
+    d.arg = d_queues + i;
+    d.n = static_cast<uint32_t>(p.nq);
+    d.pred = p.r->pred;
+    d.mode = kCollect;
+    d.chunk_begin = static_cast<uint32_t>(chunks);
+    d.order = nullptr;
+    d.qbase = 0;
+    chunks += (p.nq + plan.chunk - 1) / plan.chunk;
+    total += p.nq;
+    sl.h_descs[i] = d;
+  }
+  int rc = RTS_OK;
+  const bool sorted = want_sort(ix, total);
+  if (sorted) rc = plan_order(sl.qs, sl.h_descs, np, total, s);
+  cudaError_t e = cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, in_used, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sl.d_queues.ptr, sl.h_queues, np * sizeof(DevQueue), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sl.d_descs.ptr, sl.h_descs, np * sizeof(BatchDesc), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_counts, 0, np * sizeof(uint32_t), s);
+  if (e != cudaSuccess) rc = cuda_fail(e, "server launch staging");
+  refresh_forest(ix);
+  const BatchDesc* dd = static_cast<const BatchDesc*>(sl.d_descs.ptr);
+  if (!rc && sorted) rc = fill_order(ix, sl.qs, sl.h_descs, np > 1 ? dd : nullptr, np, total, s);
+  if (!rc)
+    rc = launch_queries(ix->forest, plan, sl.h_descs, np > 1 ? dd : nullptr, np,
+                        static_cast<uint32_t>(chunks), static_cast<uint32_t*>(sl.qs.work.ptr), s);
+  if (!rc) {
+    e = cudaEventRecord(sl.ev_kernel, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sl.h_counts, d_counts, np * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(sl.ev_counts, s);
+    if (e != cudaSuccess) rc = cuda_fail(e, "server launch");
+  }
+  if (rc) sv->fatal = rc;
+  sl.state = 1;
+  sv->launches++;
+  return true;
+}
+
+// Moves finished launches forward; returns true if anything progressed.
+bool poll_slot(rts_server* sv, Slot& sl) {
+  if (sl.state == 1) {
+    if (cudaEventQuery(sl.ev_counts) != cudaSuccess) return false;
+    auto* d_pairs = static_cast<rts_pair*>(sl.d_pairs.ptr);
+    for (size_t i = 0; i < sl.parts.size(); ++i) {
+      Part& p = sl.parts[i];
+      p.count = sl.h_counts[i];
+      if (p.count <= p.cap && p.count > 0)
+        cudaMemcpyAsync(sl.h_pairs + p.out_off, d_pairs + p.out_off, p.count * sizeof(rts_pair),
+                        cudaMemcpyDeviceToHost, sl.stream);
+    }
+    cudaEventRecord(sl.ev_pairs, sl.stream);
+    sl.state = 2;
+    return true;
+  }
+  if (sl.state == 2) {
+    if (cudaEventQuery(sl.ev_pairs) != cudaSuccess) return false;
+    for (auto& p : sl.parts) {
+      Request* r = p.r;
+      r->parts_open--;
+      if (p.count > p.cap) {  // overflow: run this part again with its exact size
+        sv->retries.push_back(Retry{r, p.q0, p.nq, p.count});
+        sv->retried++;
+        continue;
+      }
+      const uint32_t base = static_cast<uint32_t>(p.q0);
+      size_t at = r->out.size();
+      r->out.resize(at + p.count);
+      for (uint32_t k = 0; k < p.count; ++k) {
+        rts_pair x = sl.h_pairs[p.out_off + k];
+        x.query_id += base;
+        r->out[at + k] = x;
+      }
+      sv->pairs_done += p.count;
+      if (p.nq) {
+        double observed = static_cast<double>(p.count) / static_cast<double>(p.nq);
+        double& est = sv->rate[r->pred];
+        est = 0.8 * est + 0.2 * std::max(observed, 0.01);
+      }
+      if (r->parts_open == 0 && r->next == r->n) {
+        bool waiting_retry = false;
+        for (const Retry& t : sv->retries) waiting_retry |= (t.r == r);
+        if (!waiting_retry) finish_request(sv, r);
+      }
+    }
+    sl.parts.clear();
+    sl.state = 0;
+    return true;
+  }
+  return false;
+}
+
+// Applies the update request at the head of the queue.  Called only when no
+// launch is in flight and no part waits for a re-run, so every query
+// submitted before the update has its final pairs and every later query
+// launches after it (its stream waits on ev_update).
+int stage_and(cudaStream_t us, const void* host, size_t bytes, void** dev) {
+  *dev = nullptr;
+  cudaError_t e = cudaMallocAsync(dev, bytes, us);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, us);
+  if (e != cudaSuccess) return cuda_fail(e, "staging an update batch");
+  return RTS_OK;
+}
+
+void apply_update(rts_server* sv, Request* r) {
+  cudaStream_t us = sv->update_stream;
+  int rc = RTS_OK;
+  void* d = nullptr;
+  if (!r->del.empty()) {
+    rc = stage_and(us, r->del.data(), r->del.size() * sizeof(uint64_t), &d);
+    if (!rc) rc = rts_delete(sv->ix, static_cast<const uint64_t*>(d), r->del.size(), us);
+    if (d) cudaFreeAsync(d, us);
+  }
+  if (!rc && !r->upd.empty()) {
+    rc = stage_and(us, r->upd.data(), r->upd.size() * sizeof(rts_update_entry), &d);
+    if (!rc) rc = rts_update(sv->ix, static_cast<const rts_update_entry*>(d), r->upd.size(), us);
+    if (d) cudaFreeAsync(d, us);
+  }
+  if (!rc && !r->ins.empty()) {
+    const uint64_t n = r->ins.size() / 4;
+    rc = stage_and(us, r->ins.data(), n * 4 * sizeof(float), &d);
+    r->first_new_id = rts_size(sv->ix);
+    if (!rc) rc = rts_insert(sv->ix, static_cast<const float*>(d), n, us);
+    if (d) cudaFreeAsync(d, us);
+  }
+  r->status = rc;
+  cudaEventRecord(sv->ev_update, us);
+  sv->update_pending_event = true;
+  for (auto& sl : sv->slots) sl->waited_update = false;
+  sv->updates_in_flight.push_back(r);
+}
+
+void worker_loop(rts_server* sv) {
+  cudaSetDevice(sv->device);
+  std::unique_lock<std::mutex> lock(sv->mu);
+  for (;;) {
+    bool progress = false;
+    for (auto& sl : sv->slots) progress |= poll_slot(sv, *sl);
+    while (!sv->updates_in_flight.empty() &&
+           cudaEventQuery(sv->ev_update) == cudaSuccess) {
+      Request* r = sv->updates_in_flight.front();
+      sv->updates_in_flight.pop_front();
+      sv->updates_done++;
+      finish_request(sv, r);
+      progress = true;
+    }
+    // An update at the head waits until every earlier query is final.
+    bool drained = sv->retries.empty();
+    for (auto& sl : sv->slots) drained &= sl->state == 0;
+    if (!sv->pending.empty() && sv->pending.front()->is_update && drained) {
+      Request* r = sv->pending.front();
+      sv->pending.pop_front();
+      apply_update(sv, r);
+      progress = true;
+    }
+    for (auto& sl : sv->slots)
+      if (sl->state == 0 && (!sv->pending.empty() || !sv->retries.empty()) &&
+          !(sv->retries.empty() && sv->pending.front()->is_update))
+        progress |= admit_and_launch(sv, *sl);
+    bool busy = !sv->pending.empty() || !sv->retries.empty() || !sv->updates_in_flight.empty();
+    for (auto& sl : sv->slots) busy |= sl->state != 0;
+    if (sv->stop && !busy) break;
+    if (!progress) {
+      if (busy) {
+        lock.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        lock.lock();
+      } else {
+        sv->cv_work.wait_for(lock, std::chrono::milliseconds(5));
+      }
+    }
+  }
+}
+
+}  // namespace
+}  // namespace rts
+
+extern "C" {
+
+int rts_server_config_default(rts_server_config* c) {
+  if (!c) return fail(RTS_ERR_INVALID_ARGUMENT, "cfg is null");
+  std::memset(c, 0, sizeof(*c));
+  c->slots = 3;
+  c->max_parts_per_launch = 1024;
+  c->max_queries_per_launch = 1u << 20;
+  c->pairs_per_launch = 32ull << 20;
+  c->hbm_budget_bytes = 0;
+  return RTS_OK;
+}
+
+int rts_server_create(rts_index* ix, const rts_server_config* cfg, rts_server** out) {
+  if (!out) return fail(RTS_ERR_INVALID_ARGUMENT, "out is null");
+  *out = nullptr;
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  rts_server_config c;
+  if (cfg) c = *cfg; else rts_server_config_default(&c);
+  if (c.slots < 1 || c.slots > 8) return fail(RTS_ERR_INVALID_ARGUMENT, "slots must be 1..8");
+  if (c.max_parts_per_launch < 1 || c.max_queries_per_launch < 1 || c.pairs_per_launch < 1)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "launch limits must be positive");
+  // Memory budget: every slot's arena must fit in the budget (default: half
+  // of the free HBM at creation).
+  size_t free_b = 0, total_b = 0;
+  RTS_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  uint64_t budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : free_b / 2;
+  uint64_t per_slot = c.max_queries_per_launch * 16ull + c.pairs_per_launch * 8ull +
+                      c.max_queries_per_launch * 24ull + c.max_parts_per_launch * 96ull;
+  if (per_slot * c.slots > budget)
+    return fail(RTS_ERR_OUT_OF_MEMORY, "server arenas exceed the HBM budget");
+  auto sv = std::make_unique<rts_server>();
+  sv->ix = ix;
+  sv->cfg = c;
+  RTS_CUDA_TRY(cudaGetDevice(&sv->device));
+  int rc = RTS_OK;
+  for (uint32_t i = 0; i < c.slots && !rc; ++i) {
+    sv->slots.push_back(std::make_unique<Slot>());
+    rc = slot_init(sv.get(), *sv->slots.back(), c.max_queries_per_launch * 16ull,
+                   c.pairs_per_launch, c.max_parts_per_launch);
+  }
+  if (!rc) {
+    cudaError_t e = cudaStreamCreateWithFlags(&sv->update_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->ev_update, cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = cuda_fail(e, "server streams");
+  }
+  if (rc) {
+    for (auto& sl : sv->slots) slot_free(*sl);
+    return rc;
+  }
+  rts_server* raw = sv.release();
+  raw->worker = std::thread(worker_loop, raw);
+  *out = raw;
+  return RTS_OK;
+}
+
+int rts_server_destroy(rts_server* sv) {
+  if (!sv) return RTS_OK;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv_work.notify_all();
+  if (sv->worker.joinable()) sv->worker.join();
+  for (auto& sl : sv->slots) slot_free(*sl);
+  if (sv->update_stream) {
+    cudaStreamSynchronize(sv->update_stream);
+    cudaStreamDestroy(sv->update_stream);
+  }
+  if (sv->ev_update) cudaEventDestroy(sv->ev_update);
+  delete sv;
+  return RTS_OK;
+}
+
+int rts_server_submit_query(rts_server* sv, int query_kind, int predicate, const float* queries,
+                            uint64_t n, uint64_t* ticket) {
+  if (!sv || !ticket) return fail(RTS_ERR_INVALID_ARGUMENT, "server or ticket is null");
+  if (n && !queries) return fail(RTS_ERR_INVALID_ARGUMENT, "queries is null");
+  int pred;
+  uint32_t w;
+  if (query_kind == RTS_QUERY_POINTS && predicate == RTS_PREDICATE_CONTAINS) {
+    pred = kPoint;
+    w = 2;
+  } else if (query_kind == RTS_QUERY_ENVELOPES && predicate == RTS_PREDICATE_CONTAINS) {
+    pred = kContains;
+    w = 4;
+  } else if (query_kind == RTS_QUERY_ENVELOPES && predicate == RTS_PREDICATE_INTERSECTS) {
+    pred = kIntersects;
+    w = 4;
+  } else {
+    return fail(RTS_ERR_INVALID_ARGUMENT, "unsupported query kind / predicate");
+  }
+  if (n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a request");
+  auto r = std::make_unique<Request>();
+  r->pred = pred;
+  r->qwidth = w;
+  r->n = n;
+  r->q.assign(queries, queries + n * w);
+  r->t_submit = now_s();
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (sv->fatal) return fail(sv->fatal, "server stopped after an error");
+  r->ticket = sv->next_ticket++;
+  *ticket = r->ticket;
+  if (sv->t_first == 0) sv->t_first = r->t_submit;
+  Request* raw = r.get();
+  sv->reqs[r->ticket] = std::move(r);
+  if (n == 0) {
+    finish_request(sv, raw);
+  } else {
+    sv->pending.push_back(raw);
+    sv->cv_work.notify_one();
+  }
+  return RTS_OK;
+}
+
+int rts_server_submit_update(rts_server* sv, const uint64_t* delete_ids, uint64_t n_delete,
+                             const float* insert_envelopes, uint64_t n_insert,
+                             const rts_update_entry* updates, uint64_t n_update,
+                             uint64_t* ticket) {
+  if (!sv || !ticket) return fail(RTS_ERR_INVALID_ARGUMENT, "server or ticket is null");
+  if ((n_delete && !delete_ids) || (n_insert && !insert_envelopes) || (n_update && !updates))
+    return fail(RTS_ERR_INVALID_ARGUMENT, "null update array");
+  auto r = std::make_unique<Request>();
+  r->is_update = true;
+  r->del.assign(delete_ids, delete_ids + n_delete);
+  r->ins.assign(insert_envelopes, insert_envelopes + n_insert * 4);
+  r->upd.assign(updates, updates + n_update);
+  r->t_submit = now_s();
+  std::lock_guard<std::mutex> lock(sv->mu);
+  if (sv->fatal) return fail(sv->fatal, "server stopped after an error");
+  r->ticket = sv->next_ticket++;
+  *ticket = r->ticket;
+  if (sv->t_first == 0) sv->t_first = r->t_submit;
+  sv->pending.push_back(r.get());
+  sv->reqs[r->ticket] = std::move(r);
+  sv->cv_work.notify_one();
+  return RTS_OK;
+}
+
+int rts_server_wait(rts_server* sv, uint64_t ticket, double timeout_s) {
+  if (!sv) return fail(RTS_ERR_INVALID_ARGUMENT, "server is null");
+  std::unique_lock<std::mutex> lock(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return fail(RTS_ERR_INVALID_ARGUMENT, "unknown ticket");
+  Request* r = it->second.get();
+  auto until = Clock::now() + std::chrono::duration<double>(timeout_s < 0 ? 1e9 : timeout_s);
+  while (!r->done && !sv->fatal) {
+    if (sv->cv_done.wait_until(lock, until) == std::cv_status::timeout && !r->done)
+      return fail(RTS_ERR_TIMEOUT, "request not done before the timeout");
+  }
+  if (sv->fatal && !r->done) return fail(sv->fatal, "server stopped after an error");
+  return r->status;
+}
+
+int rts_server_take(rts_server* sv, uint64_t ticket, rts_pair* out, uint64_t capacity,
+                    uint64_t* n_pairs) {
+  if (!sv || !n_pairs) return fail(RTS_ERR_INVALID_ARGUMENT, "server or n_pairs is null");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return fail(RTS_ERR_INVALID_ARGUMENT, "unknown ticket");
+  Request* r = it->second.get();
+  if (!r->done) return fail(RTS_ERR_INVALID_ARGUMENT, "request not done");
+  *n_pairs = r->is_update ? r->first_new_id : r->out.size();
+  if (r->is_update) {
+    int st = r->status;
+    sv->reqs.erase(it);
+    return st;
+  }
+  if (capacity < r->out.size() || (!out && !r->out.empty()))
+    return fail(RTS_ERR_QUEUE_FULL, "output capacity smaller than the result");
+  if (!r->out.empty()) std::memcpy(out, r->out.data(), r->out.size() * sizeof(rts_pair));
+  int st = r->status;
+  sv->reqs.erase(it);
+  return st;
+}
+
+int rts_server_get_stats(rts_server* sv, rts_server_stats* st) {
+  if (!sv || !st) return fail(RTS_ERR_INVALID_ARGUMENT, "server or stats is null");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  std::memset(st, 0, sizeof(*st));
+  std::vector<double> l = sv->lat;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double q) {
+    if (l.empty()) return 0.0;
+    size_t i = static_cast<size_t>(q * static_cast<double>(l.size() - 1) + 0.5);
+    return l[std::min(i, l.size() - 1)];
+  };
+  st->requests_done = l.size();
+  st->queries_done = sv->queries_done;
+  st->pairs_done = sv->pairs_done;
+  st->launches = sv->launches;
+  st->retried_parts = sv->retried;
+  st->updates_done = sv->updates_done;
+  st->latency_p50_s = pct(0.50);
+  st->latency_p99_s = pct(0.99);
+  st->latency_max_s = l.empty() ? 0.0 : l.back();
+  st->elapsed_s = (sv->t_last > sv->t_first) ? sv->t_last - sv->t_first : 0.0;
+  return RTS_OK;
+}
+
+int rts_server_reset_stats(rts_server* sv) {
+  if (!sv) return fail(RTS_ERR_INVALID_ARGUMENT, "server is null");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  sv->lat.clear();
+  sv->queries_done = sv->pairs_done = sv->launches = sv->retried = sv->updates_done = 0;
+  sv->t_first = sv->t_last = 0;
+  return RTS_OK;
+}
+
+}  // extern "C"

@@ -101,7 +101,7 @@ __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>
 // ---------------------------------------------------------------------------
 template <int PRED, int MODE, int W>
 __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDesc& B,
-                                                 uint32_t cbeg, uint32_t cend) {
+                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf) {
   using Ops = QueryOps<PRED>;
   const uint32_t lane = lane_id();
   TravState<PRED, W> s;
@@ -114,6 +114,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
   }
   DevQueue qu{};
   if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
+  WarpOut out{wbuf, 0};
   unsigned long long cnt = 0;
 
   while (__any_sync(kFull, active)) {
@@ -146,7 +147,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       }
     }
     if (MODE == kCollect) {
-      collect_warp(qu, leafm, leafids, s.qid);
+      out.add(qu, leafm, leafids, s.qid);
     } else {
       cnt += __popc(leafm);
     }
@@ -159,6 +160,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       next = min(cend, next + __popc(idle));
     }
   }
+  if (MODE == kCollect) out.flush(qu);
   if (MODE == kCount) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
 }
 
@@ -167,7 +169,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
 // ---------------------------------------------------------------------------
 template <int PRED, int MODE, int W>
 __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc& B,
-                                               uint32_t cbeg, uint32_t cend) {
+                                               uint32_t cbeg, uint32_t cend, DevPair* wbuf) {
   using Ops = QueryOps<PRED>;
   constexpr uint32_t kTeams = 32 / W;
   constexpr uint32_t kTeamMask = (W == 32) ? kFull : ((1u << W) - 1u);
@@ -184,6 +186,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
   }
   DevQueue qu{};
   if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
+  WarpOut out{wbuf, 0};
   unsigned long long cnt = 0;
 
   while (__any_sync(kFull, active)) {
@@ -203,17 +206,8 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
       }
     }
     const uint32_t bal = __ballot_sync(kFull, hit);
-    const uint32_t leafbal = __ballot_sync(kFull, leaf_hit);
     if (MODE == kCollect) {
-      if (leafbal) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(qu.size, static_cast<uint32_t>(__popc(leafbal)));
-        base = __shfl_sync(kFull, base, 0);
-        if (leaf_hit) {
-          unsigned long long p = static_cast<unsigned long long>(base) + __popc(leafbal & lanemask_lt());
-          if (p < qu.capacity) qu.data[p] = DevPair{gid, s.qid};
-        }
-      }
+      out.add_one(qu, leaf_hit, gid, s.qid);
     } else {
       cnt += leaf_hit ? 1u : 0u;
     }
@@ -230,6 +224,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
       next = min(cend, next + __popc(idle) / W);
     }
   }
+  if (MODE == kCollect) out.flush(qu);
   if (MODE == kCount) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
 }
 

@@ -282,10 +282,29 @@ class SpatialIndex:
         check(lib().rts_query_batched(self._handle(), arr, len(batches), _stream_handle(stream)))
         self._keep = keep
 
+    def autotune(self, batches: Sequence[tuple], tune_width: bool = True, stream=None) -> dict:
+        """Times candidate launch settings on `batches` (run through internal
+        counters and queues) and keeps the fastest; see ``rts_autotune``."""
+        arr, keep = _batch_array(batches)
+        r = L.rts_tune_result()
+        check(lib().rts_autotune(self._handle(), arr, len(batches), 1 if tune_width else 0,
+                                 _stream_handle(stream), ctypes.byref(r)))
+        res = {f: getattr(r, f) for f, _ in L.rts_tune_result._fields_}
+        for k in ("node_width", "traversal", "query_occupancy", "sort_queries", "chunk"):
+            setattr(self.config, k, res[k])
+        return res
+
     def plan(self, batches: Sequence[tuple]) -> "Plan":
         """A prepared launch of fixed batches, replayable through a CUDA graph
         (``rts_plan_*``).  Query tensors and outputs must stay allocated."""
         return Plan(self, batches)
+
+    def report_query_time(self, ms: float) -> float:
+        """Feeds the refit-vs-rebuild tuner; returns the new re-sort threshold."""
+        f = ctypes.c_float()
+        check(lib().rts_report_query_time(self._handle(), float(ms), ctypes.byref(f)))
+        self.config.rebuild_update_fraction = f.value
+        return f.value
 
     # -- introspection ------------------------------------------------------------
     def size(self) -> int:

@@ -52,3 +52,26 @@ def test_plan_graph_replay(cuda, oracle, combo, order):
     cut[0:60_000:7, 3] = cut[0:60_000:7, 1]
     check(cut, True)
     plan.close()
+
+
+def test_autotune_keeps_results_and_leaves_outputs_alone(cuda, oracle):
+    rng = np.random.default_rng(78)
+    boxes = wl.clustered_boxes(rng, 80_000, 1e-2)
+    pts = wl.uniform_points(rng, 6000)
+    qs = wl.uniform_boxes(rng, 6000, 2e-2)
+    ix = rb.SpatialIndex(rb.Config(max_trees=4, rebuild_fraction=1e9))
+    for part in np.array_split(boxes, 3):
+        ix.Insert(dev(part))
+    queues = [rb.Queue(200_000) for _ in range(3)]
+    specs = [(P.kContains, dev(pts)), (P.kContains, dev(qs)), (P.kIntersects, dev(qs))]
+    batches = [(pr, q, rb.Handler.COLLECT, qu.DeviceObject()) for (pr, q), qu in zip(specs, queues)]
+    res = ix.autotune(batches, tune_width=True)
+    torch.cuda.synchronize()
+    assert all(qu.size() == 0 for qu in queues)       # the tuner used its own outputs
+    assert res["candidates"] >= 30 and res["collecting"] == 1
+    assert res["node_width"] in (4, 8, 16, 32) and res["best_ms"] <= res["first_ms"]
+    assert ix.num_trees() == 1 and ix.size() == boxes.shape[0]
+    ix.query_batched(batches)
+    torch.cuda.synchronize()
+    for (kind, q), qu in zip([(KIND_POINT, pts), (KIND_CONTAINS, qs), (KIND_INTERSECTS, qs)], queues):
+        assert_same_pairs(canon(qu.result()), oracle.run(kind, boxes, q)[2], "after autotune")
