@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--scale", type=float, default=1.0, help="scales boxes and queries (profiling)")
     ap.add_argument("--node-width", type=int, default=0)
     ap.add_argument("--traversal", type=int, default=-1)
@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch settings")
+    ap.add_argument("--rounds", type=int, default=0, help="config 4: mutation rounds (default steps)")
+    ap.add_argument("--requests", type=int, default=600, help="config 5: requests per run")
     return ap.parse_args()
 
 
@@ -93,6 +96,20 @@ def make_workload(cfg: int, scale: float, rank: int):
                 f"one launch, collecting handler")
         return dict(kind="point", pred=1, boxes=boxes, queries=pts,
                     sizes=np.array([nq], dtype=np.int64), desc=desc, qwidth=2)
+    if cfg == 4:
+        nb, nq = int(20_000_000 * scale), int(1_000_000 * scale)
+        boxes = wl.config4_base(seed=42, n_boxes=nb)
+        pts = wl.uniform_points(np.random.default_rng(1000 + rank), nq)
+        desc = f"mutable-index round queries: {nb} boxes (sides U[0,1e-3]) x {nq} points"
+        return dict(kind="point", pred=1, boxes=boxes, queries=pts,
+                    sizes=np.array([nq], dtype=np.int64), desc=desc, qwidth=2)
+    if cfg == 5:
+        nb, nq = int(50_000_000 * scale), int(1_000_000 * scale)
+        boxes = wl.config5_boxes(seed=42, n_boxes=nb)
+        queries = wl.uniform_boxes(np.random.default_rng(1000 + rank), nq, 1e-3)
+        desc = f"serving mix proxy: {nb} resident boxes x {nq} range-contains queries"
+        return dict(kind="contains", pred=1, boxes=boxes, queries=queries,
+                    sizes=np.array([nq], dtype=np.int64), desc=desc, qwidth=4)
     nb, nq = int(10_000_000 * scale), int(1_000_000 * scale)
     boxes, queries = wl.config3(seed=42, n_boxes=nb, n_queries=nq)
     if rank:
@@ -246,54 +263,63 @@ def run_reference_arm(args, rank: int, world: int):
 # ---------------------------------------------------------------------------
 # GPU leg
 # ---------------------------------------------------------------------------
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        run_reference_arm(args, rank, world)
-        return
+class Ctx:
+    """Rank, device and the timing collectives of one bench process."""
 
-    import torch
-    import torch.distributed as dist
+    def __init__(self):
+        import torch
+        import torch.distributed as dist
+        from rtspatial_b200 import replicas
+        self.torch, self.dist, self.replicas = torch, dist, replicas
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        self.dev = torch.device("cuda", self.local)
+        if self.world > 1:
+            from datetime import timedelta
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=self.dev)
 
-    import rtspatial_b200 as rb
-    from rtspatial_b200 import _lib as L
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
 
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=dev)
+    def max(self, x: float) -> float:
+        return self.replicas.max_over_ranks(x, self.dist, self.dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
-    w = make_workload(args.config, args.scale, rank)
+def make_index(args, rb):
     cfg = rb.Config()
-    if args.node_width:
-        cfg.node_width = args.node_width
-    if args.traversal >= 0:
-        cfg.traversal = args.traversal
-    if args.curve >= 0:
-        cfg.curve = args.curve
-    if args.chunk:
-        cfg.chunk = args.chunk
-    if args.sort >= 0:
-        cfg.sort_queries = args.sort
-    if args.occupancy >= 0:
-        cfg.query_occupancy = args.occupancy
-    ix = rb.SpatialIndex(cfg)
+    for k, v in (("node_width", args.node_width), ("chunk", args.chunk)):
+        if v:
+            setattr(cfg, k, v)
+    for k, v in (("traversal", args.traversal), ("curve", args.curve), ("sort_queries", args.sort),
+                 ("query_occupancy", args.occupancy)):
+        if v >= 0:
+            setattr(cfg, k, v)
+    return rb.SpatialIndex(cfg)
+
+
+def peak_hbm():
+    if os.path.exists(PEAKS_FILE):
+        with open(PEAKS_FILE) as f:
+            peaks = json.load(f)
+        if peaks.get("hbm_gbs"):
+            return float(peaks["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def run_query_bench(args, ctx):
+    """Configs 1-3: batches of one predicate over a static index."""
+    torch = ctx.torch
+    import rtspatial_b200 as rb
+    dev = ctx.dev
+    w = make_workload(args.config, args.scale, ctx.rank)
+    ix = make_index(args, rb)
     boxes_d = torch.from_numpy(w["boxes"]).to(dev)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -303,10 +329,9 @@ def main():
     del boxes_d
 
     queries_d = torch.from_numpy(w["queries"]).to(dev)
-    sizes = [int(s) for s in w["sizes"]]
+    sizes = [int(x) for x in w["sizes"]]
     offs = np.concatenate([[0], np.cumsum(sizes)])
-    nbatch = len(sizes)
-    nq = int(offs[-1])
+    nbatch, nq = len(sizes), int(offs[-1])
     qslices = [queries_d[offs[i]:offs[i + 1]] for i in range(nbatch)]
     pred = rb.Predicate(w["pred"])
 
@@ -328,69 +353,73 @@ def main():
     qobj = qobj_host.to(dev)
     batch_args = [(pred, qslices[i], rb.Handler.COLLECT, qobj[i].data_ptr()) for i in range(nbatch)]
 
+    tune = None
+    if not args.no_tune:
+        t0 = time.perf_counter()
+        tune = ix.autotune(batch_args, tune_width=True)
+        tune["seconds"] = time.perf_counter() - t0
+    plan = ix.plan(batch_args)
+
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
 
-    def l2_flush():
-        flush.fill_(1.0)
-
-    def step_batched():
+    def step_graph():
         qsize.zero_()
-        ix.query_batched(batch_args)
+        plan.launch(graph=True)
+
+    def step_nograph():
+        qsize.zero_()
+        plan.launch(graph=False)
 
     def step_plain():
         qsize.zero_()
         for i in range(nbatch):
             ix.Query(pred, qslices[i], qobj[i].data_ptr(), handler=rb.Handler.COLLECT)
 
-    stream = torch.cuda.current_stream()
-
     def timed(fn, steps):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(steps)]
-        barrier()
+        ctx.barrier()
         torch.cuda.synchronize()
         for a, b in evs:
-            l2_flush()
+            flush.fill_(1.0)
             a.record(stream)
             fn()
             b.record(stream)
         torch.cuda.synchronize()
-        barrier()
+        ctx.barrier()
         return [a.elapsed_time(b) for a, b in evs]
 
-    # parity property: batched pair multiset == plain pair multiset per batch
     def checksum():
         torch.cuda.synchronize()
         p = pairs.to(torch.int64) & 0xFFFFFFFF
         h = (p[:, 0] * 0x9E3779B1 + p[:, 1] * 0x85EBCA77) & 0xFFFFFFFFFFFF
         return int(qsize.sum().item()), int(h.sum().item())
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(ctx.local)
     clocks.start()
     for _ in range(args.warmup):
-        l2_flush()
-        step_batched()
-    torch.cuda.synchronize()
-    cs_batched = checksum()
-    t_batched = timed(step_batched, args.steps)
+        flush.fill_(1.0)
+        step_graph()
+    cs = checksum()
+    if cs[0] != total_pairs:
+        raise SystemExit(f"batched launch reported {cs[0]} pairs, counting pass {total_pairs}")
+    t_main = timed(step_graph, args.steps)
     clocks_info = clocks.stop()
-    assert cs_batched[0] == total_pairs, (cs_batched, total_pairs)
 
-    plain = None
+    forms = {}
     if not args.no_plain:
-        for _ in range(max(1, args.warmup // 2)):
-            l2_flush()
-            step_plain()
-        torch.cuda.synchronize()
-        cs_plain = checksum()
-        if cs_plain != cs_batched:
-            raise SystemExit(f"batched and plain results differ: {cs_batched} vs {cs_plain}")
-        t_plain = timed(step_plain, max(3, args.steps // 2))
-        plain_ms = max_over_ranks(sum(t_plain) / len(t_plain))
-        plain = {"value": nq * world / (plain_ms / 1000), "unit": "queries/s",
-                 "ms_per_step": plain_ms, "launches_per_step": nbatch}
+        for name, fn, k in (("batched_no_graph", step_nograph, max(3, args.steps // 2)),
+                            ("plain", step_plain, max(3, args.steps // 4))):
+            fn()
+            if checksum() != cs:
+                raise SystemExit(f"{name} results differ from the graph launch")
+            t = timed(fn, k)
+            ms = ctx.max(sum(t) / len(t))
+            forms[name] = {"value": nq * ctx.world / (ms / 1000), "unit": "queries/s",
+                           "ms_per_step": ms,
+                           "launches_per_step": nbatch if name == "plain" else 1}
 
-    # end to end through the C-ABI with host buffers
     e2e = None
     if not args.no_e2e:
         q_host = torch.from_numpy(w["queries"]).pin_memory()
@@ -399,32 +428,23 @@ def main():
 
         def step_e2e():
             queries_d.copy_(q_host, non_blocking=True)
-            step_batched()
+            step_graph()
             cnt_host.copy_(qsize, non_blocking=True)
             out_host.copy_(pairs, non_blocking=True)
 
-        for _ in range(2):
-            step_e2e()
-        t_e2e = timed(step_e2e, max(3, args.steps // 2))
-        e2e_ms = max_over_ranks(sum(t_e2e) / len(t_e2e))
-        e2e = {"value": nq * world / (e2e_ms / 1000), "unit": "queries/s",
+        step_e2e()
+        t = timed(step_e2e, max(3, args.steps // 2))
+        ms = ctx.max(sum(t) / len(t))
+        e2e = {"value": nq * ctx.world / (ms / 1000), "unit": "queries/s",
                "h2d_bytes_per_step": int(q_host.numel() * 4),
                "d2h_bytes_per_step": int(out_host.numel() * 4 + cnt_host.numel() * 4),
-               "ms_per_step": e2e_ms}
+               "ms_per_step": ms,
+               "path": "pinned H2D queries + rts_plan_launch (graph) + D2H counts and pairs"}
 
-    mean_ms = sum(t_batched) / len(t_batched)
-    step_ms = max_over_ranks(mean_ms)
-    lat = sorted(t_batched)
-    p50 = lat[len(lat) // 2]
-    p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
-
-    peaks = {}
-    if os.path.exists(PEAKS_FILE):
-        with open(PEAKS_FILE) as f:
-            peaks = json.load(f)
-    peak = peaks.get("hbm_gbs")
-    peak_src = "measured" if peak else "fallback"
-    peak = peak or FALLBACK_HBM_GBS
+    mean_ms = sum(t_main) / len(t_main)
+    step_ms = ctx.max(mean_ms)
+    lat = sorted(t_main)
+    peak, peak_src = peak_hbm()
     alg = algorithmic_bytes(w, total_pairs)
     achieved = alg / (mean_ms / 1000) / 1e9
     traffic = None
@@ -434,18 +454,18 @@ def main():
             traffic = json.load(f).get("bytes_per_launch")
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu:
         rate, n, cores, kind = cpu_query_rate(w, args.cpu_seconds, "ref")
         cpu = {"value": rate, "unit": "queries/s", "cores": cores, "kind": kind,
                "sample": f"first {n} of {nq} queries against all {w['boxes'].shape[0]} boxes, "
-                         f"uniform-grid filter, OpenMP, best of 3"}
+                         f"uniform-grid filter, OpenMP, counting only, best of 3"}
 
-    if rank == 0:
+    if ctx.rank == 0:
         line = {
             "metric": METRIC,
-            "value": nq * world / (step_ms / 1000),
+            "value": nq * ctx.world / (step_ms / 1000),
             "unit": "queries/s",
-            "n_gpus": world,
+            "n_gpus": ctx.world,
             "steps": args.steps,
             "warmup": args.warmup,
             "ms_per_step": step_ms,
@@ -457,29 +477,268 @@ def main():
             "config": {
                 "workload": w["desc"],
                 "boxes": int(w["boxes"].shape[0]), "queries": nq, "batches": nbatch,
+                "form": "rts_plan_launch replaying a captured CUDA graph (1 persistent kernel)",
                 "node_width": ix.config.node_width, "traversal": ix.config.traversal,
                 "curve": ix.config.curve, "sort_queries": ix.config.sort_queries,
                 "query_occupancy": ix.config.query_occupancy, "chunk": ix.config.chunk,
-                "l2": "flushed before every timed step (256 MiB write outside the events)",
+                "l2": "index > L2 and L2 flushed before every timed step (256 MiB write "
+                      "outside the events)",
             },
-            "pairs_per_s": total_pairs * world / (step_ms / 1000),
+            "pairs_per_s": total_pairs * ctx.world / (step_ms / 1000),
             "pairs_per_step": total_pairs,
-            "latency_ms": {"p50": p50, "p99": p99, "what": "batched step (all batches), rank 0"},
-            "plain": plain,
-            "batched_over_plain": (plain["ms_per_step"] / step_ms) if plain else None,
+            "latency_ms": {"p50": lat[len(lat) // 2],
+                           "p99": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
+                           "what": "one step (all batches), rank 0"},
+            "forms": forms,
+            "batched_over_plain": (forms["plain"]["ms_per_step"] / step_ms) if "plain" in forms else None,
+            "autotune": tune,
             "build_ms": build_ms,
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_src,
-                         "algorithmic_bytes_per_launch": alg},
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "algorithmic_bytes_per_launch": alg,
+                         "kernel": "rts::k_query (+ order sort when enabled)"},
             "cpu_baseline": cpu,
             "clocks": clocks_info,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * kernels_per_step(ix.config, nq, nbatch),
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    plan.close()
+
+
+def kernels_per_step(cfg, nq: int, nbatch: int) -> int:
+    """Kernels of this library one batched launch runs: the query kernel, plus
+    the order-key kernel and the radix sort's histogram, scan and one
+    onesweep pass per 8 key bits when queries are curve-sorted."""
+    sorted_ = cfg.sort_queries == 1 or (cfg.sort_queries == 2 and nq >= 8192)
+    if not sorted_:
+        return 1
+    end_bit = 32
+    while end_bit < 64 and (1 << (end_bit - 32)) < nbatch:
+        end_bit += 1
+    return 1 + 1 + 2 + (end_bit + 7) // 8
+
+
+def run_mutable_bench(args, ctx):
+    """Config 4: 20M boxes; each round deletes 1%, inserts 1%, updates 2%
+    (moved by U[-1e-3, 1e-3]) and answers 1M point queries.  One step = one
+    round, mutations included; the refit-vs-rebuild threshold is tuned online
+    from the measured round query times.  Every 10th round the counts are
+    checked against a freshly built index of the same boxes."""
+    torch = ctx.torch
+    import rtspatial_b200 as rb
+    from rtspatial_b200 import workloads as wl
+    dev = ctx.dev
+    n0 = int(20_000_000 * args.scale)
+    nq = int(1_000_000 * args.scale)
+    rng = np.random.default_rng(42 + ctx.rank)
+    state = wl.config4_base(seed=42, n_boxes=n0)
+    ix = make_index(args, rb)
+    ix.Insert(torch.from_numpy(state).to(dev))
+    torch.cuda.synchronize()
+    rounds = args.rounds or args.steps
+    stream = torch.cuda.current_stream()
+    counter = torch.zeros(1, dtype=torch.int64, device=dev)
+    rows, checks = [], []
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    n_live = n0
+    clocks = ClockSampler(ctx.local)
+    clocks.start()
+    total_ms = 0.0
+    for r in range(args.warmup + rounds):
+        del_ids, ins, upd_ids, upd, pts = wl.config4_round(rng, n_live, state.shape[0], nq,
+                                                            current=state)
+        d_del = torch.from_numpy(del_ids).to(dev)
+        d_ins = torch.from_numpy(ins).to(dev)
+        d_uid = torch.from_numpy(upd_ids).to(dev)
+        d_upd = torch.from_numpy(upd).to(dev)
+        d_pts = torch.from_numpy(pts).to(dev)
+        flush.fill_(1.0)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ctx.barrier()
+        torch.cuda.synchronize()
+        e[0].record(stream)
+        ix.Delete(d_del)
+        ix.Update(d_uid, d_upd)
+        ix.Insert(d_ins)
+        e[1].record(stream)
+        counter.zero_()
+        ix.Query(rb.Predicate.kContains, d_pts, counter.data_ptr(), handler=rb.Handler.COUNT)
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        maint_ms, query_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+        thr = ix.report_query_time(query_ms)
+        state[del_ids, 2] = state[del_ids, 0]
+        state[del_ids, 3] = state[del_ids, 1]
+        state[upd_ids] = upd
+        state = np.concatenate([state, ins])
+        n_live += ins.shape[0] - del_ids.shape[0]
+        got = int(counter.item())
+        if r >= args.warmup:
+            total_ms += maint_ms + query_ms
+            rows.append({"round": r - args.warmup, "maintenance_ms": maint_ms,
+                         "query_ms": query_ms, "pairs": got, "trees": ix.num_trees(),
+                         "rebuild_update_fraction": thr})
+        if r % 10 == 9 or r == args.warmup + rounds - 1:
+            fresh = rb.SpatialIndex(rb.Config(node_width=ix.config.node_width))
+            fresh.Insert(torch.from_numpy(state).to(dev))
+            c2 = torch.zeros(1, dtype=torch.int64, device=dev)
+            fresh.Query(rb.Predicate.kContains, d_pts, c2.data_ptr(), handler=rb.Handler.COUNT)
+            torch.cuda.synchronize()
+            checks.append(int(c2.item()) == got)
+            if not checks[-1]:
+                raise SystemExit(f"round {r}: mutated index {got} pairs, fresh index {int(c2.item())}")
+            del fresh
+    clocks_info = clocks.stop()
+    step_ms = ctx.max(total_ms / rounds)
+    if ctx.rank == 0:
+        q = np.array([x["query_ms"] for x in rows])
+        m = np.array([x["maintenance_ms"] for x in rows])
+        print(json.dumps({
+            "metric": METRIC, "value": nq * ctx.world / (step_ms / 1000), "unit": "queries/s",
+            "n_gpus": ctx.world, "steps": rounds, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy generators with the configuration's shapes)",
+            "config": {"workload": f"mutable index: {n0} boxes (sides U[0,1e-3]); per round 1% "
+                                   f"deletes, 1% inserts, 2% updates (moved U[-1e-3,1e-3]), "
+                                   f"{nq} uniform point queries; step = one round",
+                       "node_width": ix.config.node_width},
+            "rounds": {"query_ms_p50": float(np.median(q)), "query_ms_max": float(q.max()),
+                       "maintenance_ms_p50": float(np.median(m)),
+                       "maintenance_ms_max": float(m.max()),
+                       "final_rebuild_update_fraction": rows[-1]["rebuild_update_fraction"],
+                       "trees_max": max(x["trees"] for x in rows)},
+            "checks_vs_fresh_index": {"rounds_checked": len(checks), "all_equal": all(checks)},
+            "clocks": clocks_info,
+        }), flush=True)
+
+
+def run_serving_bench(args, ctx):
+    """Config 5: 50M resident boxes (half uniform, half clustered); requests of
+    log-uniform size in [1, 100K] (50% point, 25% contains, 25% intersects)
+    arrive as a Poisson stream at 70% of the closed-loop capacity measured
+    first, with update batches of 0.1% of the boxes interleaved (one per ten
+    requests).  Reports p50/p99 request latency (submit -> pairs on the host)
+    and the served queries/s."""
+    torch = ctx.torch
+    import rtspatial_b200 as rb
+    from rtspatial_b200 import workloads as wl
+    dev = ctx.dev
+    nb = int(50_000_000 * args.scale)
+    boxes = wl.config5_boxes(seed=42, n_boxes=nb)
+    ix = make_index(args, rb)
+    ix.Insert(torch.from_numpy(boxes).to(dev))
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(7 + ctx.rank)
+    n_req = args.requests
+
+    def make_requests(k):
+        out = []
+        for _ in range(k):
+            u = rng.random()
+            n = int(np.exp(rng.uniform(0, np.log(100_000))))
+            if u < 0.5:
+                out.append((rb.Predicate.kContains, wl.uniform_points(rng, n)))
+            elif u < 0.75:
+                out.append((rb.Predicate.kContains, wl.uniform_boxes(rng, n, 1e-3)))
+            else:
+                out.append((rb.Predicate.kIntersects, wl.uniform_boxes(rng, n, 1e-3)))
+        return out
+
+    def make_update():
+        k = max(1, int(nb * 0.001) // 3)
+        ids = rng.choice(nb, 2 * k, replace=False)
+        return dict(delete_ids=ids[:k], update_ids=ids[k:],
+                    update_boxes=wl.uniform_boxes(rng, k, 1e-3),
+                    inserts=wl.uniform_boxes(rng, k, 1e-3))
+
+    sv = rb.Server(ix, slots=3, max_queries_per_launch=1 << 19, pairs_per_launch=16 << 20)
+    # closed loop: everything submitted at once -> capacity
+    warm = make_requests(20)
+    for t in [sv.submit(p, q) for p, q in warm]:
+        sv.take(t)
+    reqs = make_requests(n_req)
+    sv.reset_stats()
+    t0 = time.perf_counter()
+    tickets = [sv.submit(p, q) for p, q in reqs]
+    for t in tickets:
+        sv.take(t)
+    closed_s = time.perf_counter() - t0
+    closed = sv.stats()
+    total_q = sum(q.shape[0] for _, q in reqs)
+    capacity_qps = total_q / closed_s
+    # open loop: Poisson arrivals at 70% of capacity, updates interleaved
+    mean_q = total_q / n_req
+    lam = 0.7 * capacity_qps / mean_q
+    reqs = make_requests(n_req)
+    gaps = rng.exponential(1.0 / lam, n_req)
+    ups = [make_update() for _ in range(n_req // 10)]
+    sv.reset_stats()
+    clocks = ClockSampler(ctx.local)
+    clocks.start()
+    t0 = time.perf_counter()
+    next_t = t0
+    tickets, up_tickets = [], []
+    for i, ((p, q), g) in enumerate(zip(reqs, gaps)):
+        next_t += g
+        while True:
+            d = next_t - time.perf_counter()
+            if d <= 0:
+                break
+            time.sleep(min(d, 0.002))
+        tickets.append(sv.submit(p, q))
+        if i % 10 == 9 and ups:
+            up_tickets.append(sv.submit_update(**ups.pop()))
+    for t in tickets:
+        sv.take(t)
+    for t in up_tickets:
+        sv.take(t)
+    open_s = time.perf_counter() - t0
+    clocks_info = clocks.stop()
+    st = sv.stats()
+    sv.close()
+    served_q = sum(q.shape[0] for _, q in reqs)
+    if ctx.rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": served_q * ctx.world / open_s, "unit": "queries/s",
+            "n_gpus": ctx.world, "steps": n_req, "warmup": 20, "ms_per_step": 1000 * open_s / n_req,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy generators with the configuration's shapes)",
+            "config": {"workload": f"serving: {nb} resident boxes (half uniform, half 64-cluster); "
+                                   f"{n_req} requests, sizes log-uniform [1,100K], 50% point / "
+                                   f"25% contains / 25% intersects, Poisson arrivals at 70% of "
+                                   f"closed-loop capacity, update batches of 0.1% every 10 requests",
+                       "slots": 3},
+            "latency_ms": {"p50": 1000 * st["latency_p50_s"], "p99": 1000 * st["latency_p99_s"],
+                           "max": 1000 * st["latency_max_s"],
+                           "what": "request submit -> its pairs on the host"},
+            "closed_loop": {"queries_per_s": capacity_qps,
+                            "p50_ms": 1000 * closed["latency_p50_s"],
+                            "p99_ms": 1000 * closed["latency_p99_s"],
+                            "launches": closed["launches"]},
+            "open_loop": {"offered_requests_per_s": lam, "launches": st["launches"],
+                          "pairs": st["pairs_done"], "retried_parts": st["retried_parts"],
+                          "updates": st["updates_done"]},
+            "clocks": clocks_info,
+        }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference_arm(args, rank, int(os.environ.get("WORLD_SIZE", "1")))
+        return
+    ctx = Ctx()
+    try:
+        if args.config in (1, 2, 3):
+            run_query_bench(args, ctx)
+        elif args.config == 4:
+            run_mutable_bench(args, ctx)
+        else:
+            run_serving_bench(args, ctx)
+    finally:
+        ctx.close()
 
 
 if __name__ == "__main__":
