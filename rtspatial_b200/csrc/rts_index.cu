@@ -34,6 +34,18 @@ int cuda_fail(cudaError_t e, const char* what) {
   return (e == cudaErrorMemoryAllocation) ? RTS_ERR_OUT_OF_MEMORY : RTS_ERR_CUDA;
 }
 
+// The stream-ordered allocator returns freed blocks to the system at every
+// synchronisation unless told otherwise; re-sorts free and reallocate
+// hundreds of MB, so keep freed blocks in the device's default pool.
+void keep_pool_memory() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+  uint64_t keep = ~0ull;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+}
+
 int buf_reserve(DevBuf& b, size_t bytes, cudaStream_t s, bool keep, size_t used) {
   if (bytes <= b.bytes && b.ptr) return RTS_OK;
   size_t cap = std::max(bytes, b.bytes + b.bytes / 2);
@@ -231,13 +243,19 @@ void refresh_forest(rts_index* ix) {
   ix->forest_dirty = false;
 }
 
-LaunchPlan plan_for(const rts_index* ix, int pred) {
+LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   LaunchPlan p;
   p.width = ix->W;
   int trav = ix->cfg.traversal;
-  if (trav == RTS_TRAVERSAL_AUTO) trav = (pred == kPoint || ix->W <= 8) ? RTS_TRAVERSAL_THREAD : RTS_TRAVERSAL_TEAM;
+  if (trav == RTS_TRAVERSAL_AUTO) trav = RTS_TRAVERSAL_THREAD;
+  (void)pred;
   p.team = (trav == RTS_TRAVERSAL_TEAM);
-  p.chunk = ix->cfg.chunk ? ix->cfg.chunk : (p.team ? 64u : 32u);
+  // Work items: the configured chunk, shrunk for small launches so that every
+  // resident warp (about 32 per SM) still gets a few chunks.
+  uint32_t chunk = ix->cfg.chunk ? ix->cfg.chunk : 128u;
+  const uint64_t warps = static_cast<uint64_t>(device_sm_count()) * 32;
+  const uint64_t fair = ((total + 4 * warps - 1) / (4 * warps) + 31) / 32 * 32;
+  p.chunk = static_cast<uint32_t>(std::max<uint64_t>(32, std::min<uint64_t>(chunk, fair)));
   p.high_occupancy = ix->cfg.query_occupancy >= 4;
   return p;
 }
@@ -320,6 +338,12 @@ int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches
   return RTS_OK;
 }
 
+uint64_t sum_queries(const rts_batch* batches, uint32_t n) {
+  uint64_t t = 0;
+  for (uint32_t i = 0; i < n; ++i) t += batches[i].n;
+  return t;
+}
+
 int check_handler(int handler, void* arg) {
   if (handler != RTS_HANDLER_COUNT && handler != RTS_HANDLER_COLLECT)
     return fail(RTS_ERR_INVALID_ARGUMENT, "unknown handler");
@@ -349,7 +373,7 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
     if ((rc = plan_order(ix->qs, &b, 1, n, s))) return rc;
     if ((rc = fill_order(ix, ix->qs, &b, nullptr, 1, n, s))) return rc;
   }
-  LaunchPlan plan = plan_for(ix, pred);
+  LaunchPlan plan = plan_for(ix, pred, n);
   uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
   return launch_queries(ix->forest, plan, &b, nullptr, 1, static_cast<uint32_t>(chunks),
                         static_cast<uint32_t*>(ix->qs.work.ptr), s);
@@ -402,6 +426,7 @@ int rts_create(const rts_config* cfg, rts_index** out) {
     return fail(RTS_ERR_INVALID_ARGUMENT, "max_trees must be in 1..16");
   auto* ix = new (std::nothrow) rts_index();
   if (!ix) return fail(RTS_ERR_OUT_OF_MEMORY, "host allocation failed");
+  keep_pool_memory();
   ix->cfg = c;
   ix->W = c.node_width;
   if (c.preallocate && c.max_geometries) {
@@ -536,7 +561,7 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   if (n_batches == 0) return RTS_OK;
   if (!batches) return fail(RTS_ERR_INVALID_ARGUMENT, "batches is null");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  LaunchPlan plan = plan_for(ix, kContains);
+  LaunchPlan plan = plan_for(ix, kContains, sum_queries(batches, n_batches));
   std::vector<BatchDesc> descs;
   uint64_t chunks = 0;
   int rc = make_descs(ix, batches, n_batches, plan, descs, chunks);
@@ -680,7 +705,7 @@ extern "C" int rts_query_batched_noalloc(rts_index* ix, const rts_batch* batches
   uint32_t nd = 0;
   uint64_t chunks = 0;
   int rc;
-  LaunchPlan plan = plan_for(ix, kContains);
+  LaunchPlan plan = plan_for(ix, kContains, sum_queries(batches, n_batches));
   for (uint32_t i = 0; i < n_batches; ++i) {
     const rts_batch& b = batches[i];
     if ((rc = check_handler(b.handler, b.arg))) return rc;

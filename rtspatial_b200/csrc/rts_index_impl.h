@@ -111,7 +111,9 @@ inline uint64_t round_up(uint64_t a, uint64_t b) { return (a + b - 1) / b * b; }
 void refresh_forest(rts_index* ix);
 // Re-sorts every box of the index into one tree at the index's node width.
 int rebuild_all(rts_index* ix, cudaStream_t s);
-LaunchPlan plan_for(const rts_index* ix, int pred);
+LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total_queries);
+uint64_t sum_queries(const rts_batch* batches, uint32_t n);
+void keep_pool_memory();
 bool want_sort(const rts_index* ix, uint64_t total);
 int check_handler(int handler, void* arg);
 int plan_order(QueryScratch& qs, BatchDesc* descs, uint32_t nd, uint64_t total, cudaStream_t s);

@@ -96,6 +96,8 @@ struct LaunchPlan {
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
                    uint32_t* work_counter, cudaStream_t s);
+// Number of SMs of the current device (cached).
+int device_sm_count();
 // Resident CTAs per SM of the chosen query kernel (for sizing the grid).
 int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks);
 

@@ -64,7 +64,7 @@ int rts_plan_create(rts_index* ix, const rts_batch* batches, uint32_t n_batches,
   auto* p = new (std::nothrow) rts_plan();
   if (!p) return fail(RTS_ERR_OUT_OF_MEMORY, "host allocation failed");
   p->ix = ix;
-  p->plan = plan_for(ix, kContains);
+  p->plan = plan_for(ix, kContains, n_batches ? sum_queries(batches, n_batches) : 0);
   int rc = make_descs(ix, batches, n_batches, p->plan, p->descs, p->chunks);
   cudaStream_t s = 0;
   for (const auto& d : p->descs) p->total += d.n;

@@ -108,15 +108,20 @@ static QueryKernel pick_kernel(const LaunchPlan& p) {
 
 static int g_num_sms = 0;
 
+int device_sm_count() {
+  if (g_num_sms == 0) {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    g_num_sms = n > 0 ? n : 1;
+  }
+  return g_num_sms;
+}
+
 int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks) {
   QueryKernel k = pick_kernel(plan);
   if (!k) return 0;
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 1;
-  }
+  device_sm_count();
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kQueryThreads, 0);
   if (per_sm <= 0) per_sm = 1;

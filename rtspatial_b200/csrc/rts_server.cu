@@ -269,7 +269,9 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
   auto* d_pairs = static_cast<DevPair*>(sl.d_pairs.ptr);
   auto* d_counts = static_cast<uint32_t*>(sl.d_counts.ptr);
   auto* d_queues = static_cast<DevQueue*>(sl.d_queues.ptr);
-  LaunchPlan plan = plan_for(ix, kContains);
+  uint64_t total_q = 0;
+  for (const Part& p : sl.parts) total_q += p.nq;
+  LaunchPlan plan = plan_for(ix, kContains, total_q);
   uint64_t chunks = 0, total = 0;
   for (uint32_t i = 0; i < np; ++i) {
     const Part& p = sl.parts[i];
@@ -284,6 +286,7 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
     d.chunk_begin = static_cast<uint32_t>(chunks);
     d.order = nullptr;
     d.qbase = 0;
+    d.id_offset = static_cast<uint32_t>(p.q0);  // ids relative to the request
     chunks += (p.nq + plan.chunk - 1) / plan.chunk;
     total += p.nq;
     sl.h_descs[i] = d;
@@ -343,14 +346,10 @@ bool poll_slot(rts_server* sv, Slot& sl) {
         sv->retried++;
         continue;
       }
-      const uint32_t base = static_cast<uint32_t>(p.q0);
       size_t at = r->out.size();
       r->out.resize(at + p.count);
-      for (uint32_t k = 0; k < p.count; ++k) {
-        rts_pair x = sl.h_pairs[p.out_off + k];
-        x.query_id += base;
-        r->out[at + k] = x;
-      }
+      if (p.count)
+        std::memcpy(r->out.data() + at, sl.h_pairs + p.out_off, p.count * sizeof(rts_pair));
       sv->pairs_done += p.count;
       if (p.nq) {
         double observed = static_cast<double>(p.count) / static_cast<double>(p.nq);

@@ -29,7 +29,7 @@ struct BatchDesc {
   uint32_t chunk_begin;   // index of the batch's first chunk in the launch
   const uint32_t* order;  // optional visiting order (query ids), or nullptr
   uint32_t qbase;         // offset of the batch in the launch's concatenated order
-  uint32_t pad;
+  uint32_t id_offset;     // added to every reported query id (0 for a Query call)
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -147,7 +147,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       }
     }
     if (MODE == kCollect) {
-      out.add(qu, leafm, leafids, s.qid);
+      out.add(qu, leafm, leafids, s.qid + B.id_offset);
     } else {
       cnt += __popc(leafm);
     }
@@ -207,7 +207,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
     }
     const uint32_t bal = __ballot_sync(kFull, hit);
     if (MODE == kCollect) {
-      out.add_one(qu, leaf_hit, gid, s.qid);
+      out.add_one(qu, leaf_hit, gid, s.qid + B.id_offset);
     } else {
       cnt += leaf_hit ? 1u : 0u;
     }

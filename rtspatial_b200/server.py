@@ -66,7 +66,7 @@ class Server:
             return np.zeros((0, 2), dtype=np.uint32) if n.value == 0 else n.value
         if rc != L.RTS_ERR_QUEUE_FULL:
             check(rc)
-        out = np.zeros((n.value, 2), dtype=np.uint32)
+        out = np.empty((n.value, 2), dtype=np.uint32)
         check(lib().rts_server_take(self._h, ticket, out.ctypes.data, n.value, ctypes.byref(n)))
         return out
 
