@@ -185,9 +185,15 @@ __device__ __forceinline__ float2 root_magnitude(float4 r) {
 template <int PRED>
 struct QueryOps;
 
+// node():   test of an upper-level entry (a hull);
+// leaf():   exact predicate on a stored box;
+// coarse(): a test valid at both levels that implies nothing is missed;
+// kRefine:  leaves that pass coarse() still need the exact test.
 template <>
 struct QueryOps<kPoint> {
   using Q = float2;
+  static constexpr bool kRefine = false;
+  static __device__ __forceinline__ bool coarse(float4 e, const Q& p) { return contains_point(e, p); }
   static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
     return reinterpret_cast<const float2*>(qs)[i];
   }
@@ -199,6 +205,8 @@ struct QueryOps<kPoint> {
 template <>
 struct QueryOps<kContains> {
   using Q = float4;
+  static constexpr bool kRefine = false;
+  static __device__ __forceinline__ bool coarse(float4 e, const Q& q) { return contains_box(e, q); }
   static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
     return reinterpret_cast<const float4*>(qs)[i];
   }
@@ -211,6 +219,12 @@ struct QueryOps<kContains> {
 template <>
 struct QueryOps<kIntersects> {
   using Q = IsectQuery;
+  static constexpr bool kRefine = true;
+  static __device__ __forceinline__ bool coarse(float4 e, const Q& q) {
+    return overlaps(make_float4(fminf(e.x, e.z), fminf(e.y, e.w), fmaxf(e.x, e.z), fmaxf(e.y, e.w)),
+                    q.nb);
+  }
+  static __device__ __forceinline__ bool exact(float4 g, const Q& q) { return isect_exact(g, q); }
   static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
     return make_isect_query(reinterpret_cast<const float4*>(qs)[i]);
   }

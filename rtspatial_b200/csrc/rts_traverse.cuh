@@ -121,28 +121,28 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
     uint32_t leafm = 0;
     const uint32_t* leafids = nullptr;
     if (active) {
+      // One load-and-test path for leaves and nodes (no divergent copies).
       const TreeDesc& T = F.tree[s.t];
       const uint32_t first = s.g * W;
-      if (s.L == 0) {
-        const float4* p = T.leaves + first;
-        const uint32_t lim = T.n - first;
-        float4 e[W];
+      const bool at_leaf = (s.L == 0);
+      const float4* p = at_leaf ? T.leaves + first : T.nodes + T.level_off[s.L] + first;
+      const uint32_t lim = (at_leaf ? T.n : T.level_cnt[s.L]) - first;
+      float4 e[W];
 #pragma unroll
-        for (int c = 0; c < W; ++c) e[c] = __ldg(p + c);
+      for (int c = 0; c < W; ++c) e[c] = __ldg(p + c);
+      uint32_t m = 0;
 #pragma unroll
-        for (int c = 0; c < W; ++c)
-          if (static_cast<uint32_t>(c) < lim && Ops::leaf(e[c], s.q)) leafm |= 1u << c;
+      for (int c = 0; c < W; ++c)
+        if (static_cast<uint32_t>(c) < lim && Ops::coarse(e[c], s.q)) m |= 1u << c;
+      if (at_leaf) {
+        if constexpr (Ops::kRefine) {
+#pragma unroll
+          for (int c = 0; c < W; ++c)
+            if (((m >> c) & 1u) && !Ops::exact(e[c], s.q)) m &= ~(1u << c);
+        }
+        leafm = m;
         leafids = T.ids + first;
       } else {
-        const float4* p = T.nodes + T.level_off[s.L] + first;
-        const uint32_t lim = T.level_cnt[s.L] - first;
-        float4 e[W];
-#pragma unroll
-        for (int c = 0; c < W; ++c) e[c] = __ldg(p + c);
-        uint32_t m = 0;
-#pragma unroll
-        for (int c = 0; c < W; ++c)
-          if (static_cast<uint32_t>(c) < lim && Ops::node(e[c], s.q)) m |= 1u << c;
         s.ms.set(s.L, m);
       }
     }
