@@ -251,6 +251,7 @@ typedef struct rts_server_config {
   uint64_t max_queries_per_launch; /* query capacity of one launch arena */
   uint64_t pairs_per_launch;       /* pair capacity of one launch arena */
   uint64_t hbm_budget_bytes;       /* bound on all arenas (0 = half the free HBM) */
+  uint64_t host_result_bytes;      /* pinned host memory holding results until taken */
 } rts_server_config;
 typedef struct rts_server_stats {
   uint64_t requests_done, queries_done, pairs_done, launches, retried_parts, updates_done;

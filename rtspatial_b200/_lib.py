@@ -86,7 +86,7 @@ class rts_batch(ctypes.Structure):
 class rts_server_config(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("max_parts_per_launch", ctypes.c_uint32),
                 ("max_queries_per_launch", ctypes.c_uint64), ("pairs_per_launch", ctypes.c_uint64),
-                ("hbm_budget_bytes", ctypes.c_uint64)]
+                ("hbm_budget_bytes", ctypes.c_uint64), ("host_result_bytes", ctypes.c_uint64)]
 
 
 class rts_server_stats(ctypes.Structure):

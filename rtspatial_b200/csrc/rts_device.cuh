@@ -322,7 +322,10 @@ struct WarpOut {
     n = 0;
   }
 
-  // Adds, for every lane, (ids[c], qid) for each set bit c of m.
+  // Adds, for every lane, (ids[c], qid) for each set bit c of m (c < W).
+  // The id loads are unrolled and predicated so they are all in flight at
+  // once instead of one dependent load per pair.
+  template <int W>
   __device__ __forceinline__ void add(const DevQueue& qu, uint32_t m, const uint32_t* ids,
                                       uint32_t qid) {
     if (!__any_sync(kFull, m != 0)) return;
@@ -340,21 +343,20 @@ struct WarpOut {
       uint32_t base = 0;
       if (lane == 31) base = atomicAdd(qu.size, total);
       base = __shfl_sync(kFull, base, 31);
-      unsigned long long p = static_cast<unsigned long long>(base) + (incl - cnt);
-      while (m) {
-        int c = __ffs(m) - 1;
-        m &= m - 1;
-        if (p < qu.capacity) qu.data[p] = DevPair{ids[c], qid};
-        ++p;
+      const unsigned long long p0 = static_cast<unsigned long long>(base) + (incl - cnt);
+#pragma unroll
+      for (int c = 0; c < W; ++c) {
+        if ((m >> c) & 1u) {
+          unsigned long long p = p0 + __popc(m & ((1u << c) - 1u));
+          if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + c), qid};
+        }
       }
       return;
     }
-    uint32_t at = n + incl - cnt;
-    while (m) {
-      int c = __ffs(m) - 1;
-      m &= m - 1;
-      buf[at++] = DevPair{ids[c], qid};
-    }
+    const uint32_t at = n + incl - cnt;
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+      if ((m >> c) & 1u) buf[at + __popc(m & ((1u << c) - 1u))] = DevPair{__ldg(ids + c), qid};
     n += total;
   }
 

@@ -21,6 +21,7 @@
 // mix; the engine shifts ids by the part's offset in its request.
 #include <chrono>
 #include <condition_variable>
+#include <map>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -38,6 +39,64 @@ double now_s() {
   return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
 }
 
+// Pinned host memory that receives every part's pairs straight from the
+// device (one DMA, no staging copy); rts_server_take copies them out and
+// frees them.  First fit over a free list, 256-byte granules.  A full arena
+// holds finished launches back until results are taken (back-pressure).
+struct PinnedArena {
+  unsigned char* base = nullptr;
+  size_t bytes = 0;
+  std::map<size_t, size_t> free_;  // offset -> size
+
+  int init(size_t n) {
+    n = (n + 255) & ~size_t(255);
+    RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&base), n));
+    bytes = n;
+    free_.clear();
+    free_[0] = n;
+    return RTS_OK;
+  }
+  void destroy() {
+    if (base) cudaFreeHost(base);
+    base = nullptr;
+  }
+  bool alloc(size_t n, size_t* off) {
+    n = (n + 255) & ~size_t(255);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      *off = it->first;
+      size_t rest = it->second - n;
+      size_t at = it->first + n;
+      free_.erase(it);
+      if (rest) free_[at] = rest;
+      return true;
+    }
+    return false;
+  }
+  void release(size_t off, size_t n) {
+    n = (n + 255) & ~size_t(255);
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct Chunk {
+  size_t off;     // byte offset in the arena, or ~0 when held in `heap`
+  uint64_t n;     // pairs
+  std::vector<rts_pair> heap;
+};
+
 struct Request {
   uint64_t ticket = 0;
   bool is_update = false;
@@ -47,7 +106,8 @@ struct Request {
   uint64_t n = 0;               // queries
   uint64_t next = 0;            // first query not yet admitted
   uint64_t parts_open = 0;      // admitted parts whose pairs are not back yet
-  std::vector<rts_pair> out;
+  std::vector<Chunk> out;        // pairs, part by part
+  uint64_t n_out = 0;
   std::vector<uint64_t> del;
   std::vector<float> ins;
   std::vector<rts_update_entry> upd;
@@ -64,6 +124,8 @@ struct Part {
   uint64_t out_off = 0;         // pair offset in the slot's pair buffer
   uint64_t cap = 0;             // pairs reserved
   uint32_t count = 0;           // pairs reported
+  size_t host_off = 0;          // arena offset of the pairs once copied
+  bool heap = false;            // too large for the arena: copied to the heap
 };
 
 struct Retry {
@@ -98,6 +160,7 @@ struct rts_server {
   rts_server_config cfg{};
   int device = 0;
   std::vector<std::unique_ptr<Slot>> slots;
+  PinnedArena arena;
   cudaStream_t update_stream = nullptr;
   cudaEvent_t ev_update = nullptr;
   bool update_pending_event = false;  // ev_update recorded; slots must wait on it once
@@ -324,13 +387,36 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
 bool poll_slot(rts_server* sv, Slot& sl) {
   if (sl.state == 1) {
     if (cudaEventQuery(sl.ev_counts) != cudaSuccess) return false;
-    auto* d_pairs = static_cast<rts_pair*>(sl.d_pairs.ptr);
+    // Reserve arena space for every part that fits its capacity; if the arena
+    // is full, try again later (results not yet taken hold it).
+    std::vector<size_t> got;
+    bool ok = true;
     for (size_t i = 0; i < sl.parts.size(); ++i) {
       Part& p = sl.parts[i];
       p.count = sl.h_counts[i];
-      if (p.count <= p.cap && p.count > 0)
-        cudaMemcpyAsync(sl.h_pairs + p.out_off, d_pairs + p.out_off, p.count * sizeof(rts_pair),
-                        cudaMemcpyDeviceToHost, sl.stream);
+      p.heap = false;
+      if (p.count > p.cap || p.count == 0) continue;
+      const size_t bytes = p.count * sizeof(rts_pair);
+      if (bytes > sv->arena.bytes) {
+        p.heap = true;
+        continue;
+      }
+      if (!sv->arena.alloc(bytes, &p.host_off)) {
+        ok = false;
+        break;
+      }
+      got.push_back(i);
+    }
+    if (!ok) {
+      for (size_t i : got)
+        sv->arena.release(sl.parts[i].host_off, sl.parts[i].count * sizeof(rts_pair));
+      return false;
+    }
+    auto* d_pairs = static_cast<rts_pair*>(sl.d_pairs.ptr);
+    for (auto& p : sl.parts) {
+      if (p.count > p.cap || p.count == 0 || p.heap) continue;
+      cudaMemcpyAsync(sv->arena.base + p.host_off, d_pairs + p.out_off,
+                      p.count * sizeof(rts_pair), cudaMemcpyDeviceToHost, sl.stream);
     }
     cudaEventRecord(sl.ev_pairs, sl.stream);
     sl.state = 2;
@@ -338,6 +424,7 @@ bool poll_slot(rts_server* sv, Slot& sl) {
   }
   if (sl.state == 2) {
     if (cudaEventQuery(sl.ev_pairs) != cudaSuccess) return false;
+    auto* d_pairs = static_cast<rts_pair*>(sl.d_pairs.ptr);
     for (auto& p : sl.parts) {
       Request* r = p.r;
       r->parts_open--;
@@ -346,10 +433,20 @@ bool poll_slot(rts_server* sv, Slot& sl) {
         sv->retried++;
         continue;
       }
-      size_t at = r->out.size();
-      r->out.resize(at + p.count);
-      if (p.count)
-        std::memcpy(r->out.data() + at, sl.h_pairs + p.out_off, p.count * sizeof(rts_pair));
+      if (p.count) {
+        Chunk c;
+        c.n = p.count;
+        if (p.heap) {
+          c.off = ~size_t(0);
+          c.heap.resize(p.count);
+          cudaMemcpy(c.heap.data(), d_pairs + p.out_off, p.count * sizeof(rts_pair),
+                     cudaMemcpyDeviceToHost);
+        } else {
+          c.off = p.host_off;
+        }
+        r->out.push_back(std::move(c));
+        r->n_out += p.count;
+      }
       sv->pairs_done += p.count;
       if (p.nq) {
         double observed = static_cast<double>(p.count) / static_cast<double>(p.nq);
@@ -367,6 +464,12 @@ bool poll_slot(rts_server* sv, Slot& sl) {
     return true;
   }
   return false;
+}
+
+void release_chunks(rts_server* sv, Request* r) {
+  for (auto& c : r->out)
+    if (c.off != ~size_t(0)) sv->arena.release(c.off, c.n * sizeof(rts_pair));
+  r->out.clear();
 }
 
 // Applies the update request at the head of the queue.  Called only when no
@@ -464,6 +567,7 @@ int rts_server_config_default(rts_server_config* c) {
   c->max_queries_per_launch = 1u << 20;
   c->pairs_per_launch = 32ull << 20;
   c->hbm_budget_bytes = 0;
+  c->host_result_bytes = 1ull << 30;
   return RTS_OK;
 }
 
@@ -495,6 +599,7 @@ int rts_server_create(rts_index* ix, const rts_server_config* cfg, rts_server** 
     rc = slot_init(sv.get(), *sv->slots.back(), c.max_queries_per_launch * 16ull,
                    c.pairs_per_launch, c.max_parts_per_launch);
   }
+  if (!rc) rc = sv->arena.init(c.host_result_bytes ? c.host_result_bytes : (1ull << 30));
   if (!rc) {
     cudaError_t e = cudaStreamCreateWithFlags(&sv->update_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->ev_update, cudaEventDisableTiming);
@@ -502,6 +607,7 @@ int rts_server_create(rts_index* ix, const rts_server_config* cfg, rts_server** 
   }
   if (rc) {
     for (auto& sl : sv->slots) slot_free(*sl);
+    sv->arena.destroy();
     return rc;
   }
   rts_server* raw = sv.release();
@@ -524,6 +630,8 @@ int rts_server_destroy(rts_server* sv) {
     cudaStreamDestroy(sv->update_stream);
   }
   if (sv->ev_update) cudaEventDestroy(sv->ev_update);
+  sv->reqs.clear();
+  sv->arena.destroy();
   delete sv;
   return RTS_OK;
 }
@@ -616,15 +724,22 @@ int rts_server_take(rts_server* sv, uint64_t ticket, rts_pair* out, uint64_t cap
   if (it == sv->reqs.end()) return fail(RTS_ERR_INVALID_ARGUMENT, "unknown ticket");
   Request* r = it->second.get();
   if (!r->done) return fail(RTS_ERR_INVALID_ARGUMENT, "request not done");
-  *n_pairs = r->is_update ? r->first_new_id : r->out.size();
+  *n_pairs = r->is_update ? r->first_new_id : r->n_out;
   if (r->is_update) {
     int st = r->status;
     sv->reqs.erase(it);
     return st;
   }
-  if (capacity < r->out.size() || (!out && !r->out.empty()))
+  if (capacity < r->n_out || (!out && r->n_out))
     return fail(RTS_ERR_QUEUE_FULL, "output capacity smaller than the result");
-  if (!r->out.empty()) std::memcpy(out, r->out.data(), r->out.size() * sizeof(rts_pair));
+  uint64_t at = 0;
+  for (auto& c : r->out) {
+    const rts_pair* src = (c.off == ~size_t(0)) ? c.heap.data()
+                                                : reinterpret_cast<const rts_pair*>(sv->arena.base + c.off);
+    std::memcpy(out + at, src, c.n * sizeof(rts_pair));
+    at += c.n;
+  }
+  release_chunks(sv, r);
   int st = r->status;
   sv->reqs.erase(it);
   return st;

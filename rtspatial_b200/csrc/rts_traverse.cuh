@@ -147,7 +147,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       }
     }
     if (MODE == kCollect) {
-      out.add(qu, leafm, leafids, s.qid + B.id_offset);
+      out.template add<W>(qu, leafm, leafids, s.qid + B.id_offset);
     } else {
       cnt += __popc(leafm);
     }

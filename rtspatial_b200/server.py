@@ -14,7 +14,7 @@ from ._lib import check, lib
 class Server:
     def __init__(self, index, slots: int = 3, max_queries_per_launch: int = 1 << 20,
                  pairs_per_launch: int = 32 << 20, max_parts_per_launch: int = 1024,
-                 hbm_budget_bytes: int = 0):
+                 hbm_budget_bytes: int = 0, host_result_bytes: int = 1 << 30):
         c = L.rts_server_config()
         check(lib().rts_server_config_default(ctypes.byref(c)))
         c.slots = slots
@@ -22,6 +22,7 @@ class Server:
         c.pairs_per_launch = pairs_per_launch
         c.max_parts_per_launch = max_parts_per_launch
         c.hbm_budget_bytes = hbm_budget_bytes
+        c.host_result_bytes = host_result_bytes
         self.index = index
         self._h = ctypes.c_void_p()
         check(lib().rts_server_create(index._handle(), ctypes.byref(c), ctypes.byref(self._h)))
@@ -56,9 +57,10 @@ class Server:
     def wait(self, ticket: int, timeout: float = -1.0) -> None:
         check(lib().rts_server_wait(self._h, ticket, timeout))
 
-    def take(self, ticket: int) -> np.ndarray:
+    def take(self, ticket: int, out: np.ndarray | None = None) -> np.ndarray:
         """(R, 2) uint32 (geom_id, query_id) of a query request (waits for it);
-        for an update request, the first id its inserts received."""
+        for an update request, the first id its inserts received.  `out`, when
+        given and large enough, receives the pairs (a view of it is returned)."""
         self.wait(ticket)
         n = ctypes.c_uint64()
         rc = lib().rts_server_take(self._h, ticket, None, 0, ctypes.byref(n))
@@ -66,9 +68,10 @@ class Server:
             return np.zeros((0, 2), dtype=np.uint32) if n.value == 0 else n.value
         if rc != L.RTS_ERR_QUEUE_FULL:
             check(rc)
-        out = np.empty((n.value, 2), dtype=np.uint32)
+        if out is None or out.shape[0] < n.value:
+            out = np.empty((n.value, 2), dtype=np.uint32)
         check(lib().rts_server_take(self._h, ticket, out.ctypes.data, n.value, ctypes.byref(n)))
-        return out
+        return out[:n.value]
 
     def stats(self) -> dict:
         st = L.rts_server_stats()
