@@ -61,6 +61,7 @@ struct Config {
   uint32_t chunk = 0;
   int sort_queries = 2;
   int query_occupancy = 0;
+  float frontier_factor = 0.0f;
 };
 
 template <typename COORD_T, int N_DIMS>
@@ -104,6 +105,7 @@ class SpatialIndex {
     c.chunk = config.chunk;
     c.sort_queries = config.sort_queries;
     c.query_occupancy = config.query_occupancy;
+    c.frontier_factor = config.frontier_factor;
     if (h_) rts_destroy(h_);
     h_ = nullptr;
     RTS_CHECK(rts_create(&c, &h_));

@@ -113,12 +113,15 @@ typedef struct rts_config {
                                     above which Update re-sorts instead of refitting */
   uint32_t chunk;         /* queries per device work item (0 = library default) */
   int32_t query_occupancy; /* 0 library default; 4: query kernel capped at 64 registers */
-  int32_t reserved0;
+  float frontier_factor;   /* frontier traversal: entries per query of each level buffer
+                              (queries beyond it are answered depth-first); 0 = 16 */
 } rts_config;
 
 #define RTS_TRAVERSAL_AUTO 0
 #define RTS_TRAVERSAL_THREAD 1 /* one thread per query, loops over a node's children */
 #define RTS_TRAVERSAL_TEAM 2   /* node_width lanes per query, one child per lane */
+#define RTS_TRAVERSAL_FRONTIER 3 /* level by level over the whole launch (batches of one
+                                    predicate and handler; others run depth-first) */
 
 #define RTS_CURVE_MORTON 0
 #define RTS_CURVE_HILBERT 1

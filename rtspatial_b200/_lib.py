@@ -28,6 +28,7 @@ RTS_HANDLER_COLLECT = 1
 RTS_TRAVERSAL_AUTO = 0
 RTS_TRAVERSAL_THREAD = 1
 RTS_TRAVERSAL_TEAM = 2
+RTS_TRAVERSAL_FRONTIER = 3
 RTS_CURVE_MORTON = 0
 RTS_CURVE_HILBERT = 1
 RTS_QUERY_POINTS = 0
@@ -58,7 +59,7 @@ class rts_config(ctypes.Structure):
         ("rebuild_update_fraction", ctypes.c_float),
         ("chunk", ctypes.c_uint32),
         ("query_occupancy", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("frontier_factor", ctypes.c_float),
     ]
 
 

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librtspatial_b200.so")
-SOURCES = ["rts_index.cu", "rts_plan.cu", "rts_server.cu", "rts_tune.cu", "rts_query.cu", "rts_build.cu"]
+SOURCES = ["rts_index.cu", "rts_plan.cu", "rts_server.cu", "rts_tune.cu", "rts_frontier.cu", "rts_query.cu", "rts_build.cu"]
 HEADERS = ["rts_device.cuh", "rts_traverse.cuh", "rts_internal.h", "rts_index_impl.h"]
 
 NVCC_FLAGS = [

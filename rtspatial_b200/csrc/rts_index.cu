@@ -249,6 +249,7 @@ LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   int trav = ix->cfg.traversal;
   if (trav == RTS_TRAVERSAL_AUTO) trav = RTS_TRAVERSAL_THREAD;
   (void)pred;
+  p.frontier = (trav == RTS_TRAVERSAL_FRONTIER);
   p.team = (trav == RTS_TRAVERSAL_TEAM);
   // Work items: the configured chunk, shrunk for small launches so that every
   // resident warp (about 32 per SM) still gets a few chunks.
@@ -302,6 +303,7 @@ int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches
   out.clear();
   out.reserve(n_batches);
   chunks = 0;
+  uint64_t qsum = 0;
   int rc;
   (void)ix;
   for (uint32_t i = 0; i < n_batches; ++i) {
@@ -330,12 +332,63 @@ int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches
     d.mode = b.handler;
     d.chunk_begin = static_cast<uint32_t>(chunks);
     d.order = nullptr;
-    d.qbase = 0;
+    d.qbase = static_cast<uint32_t>(qsum);
+    qsum += b.n;
+    if (qsum > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a launch");
     chunks += (b.n + plan.chunk - 1) / plan.chunk;
     if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
     out.push_back(d);
   }
   return RTS_OK;
+}
+
+int reserve_frontier(rts_index* ix, QueryScratch& qs, uint64_t total, cudaStream_t s) {
+  const double f = ix->cfg.frontier_factor > 0 ? ix->cfg.frontier_factor : 16.0;
+  uint64_t cap = static_cast<uint64_t>(f * static_cast<double>(total)) + 4096;
+  cap = std::min<uint64_t>(cap, 0x7fffffffull / 2);
+  int rc;
+  if ((rc = buf_reserve(qs.fr_qbuf, total * 16, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_qaux, total * 16, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_qbatch, total * 4, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_vis, total * 4, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_a, cap * 8, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_b, cap * 8, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_counts, kMaxLevels * sizeof(uint32_t), s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_spill, ((total + 31) / 32) * 4 + 4, s, false, 0)) ||
+      (rc = buf_reserve(qs.fr_any, 4, s, false, 0)))
+    return rc;
+  FrontierBufs& fb = qs.fb;
+  fb.qbuf = qs.fr_qbuf.ptr;
+  fb.qaux = qs.fr_qaux.ptr;
+  fb.qbatch = static_cast<uint32_t*>(qs.fr_qbatch.ptr);
+  fb.vis = static_cast<uint32_t*>(qs.fr_vis.ptr);
+  fb.fa = qs.fr_a.ptr;
+  fb.fb = qs.fr_b.ptr;
+  fb.cap = static_cast<uint32_t>(std::min<uint64_t>(qs.fr_a.bytes, qs.fr_b.bytes) / 8);
+  fb.counts = static_cast<uint32_t*>(qs.fr_counts.ptr);
+  fb.counts_cap = qs.fr_counts.bytes / 4;
+  fb.spill = static_cast<uint32_t*>(qs.fr_spill.ptr);
+  fb.any_spill = static_cast<uint32_t*>(qs.fr_any.ptr);
+  return RTS_OK;
+}
+
+int run_launch(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const BatchDesc* descs,
+               const BatchDesc* dd, uint32_t nd, uint64_t total, uint64_t chunks, cudaStream_t s) {
+  bool uniform = plan.frontier && nd > 0;
+  for (uint32_t i = 1; i < nd && uniform; ++i)
+    uniform = descs[i].pred == descs[0].pred && descs[i].mode == descs[0].mode;
+  auto* work = static_cast<uint32_t*>(qs.work.ptr);
+  if (!uniform)
+    return launch_queries(ix->forest, plan, descs, dd, nd, static_cast<uint32_t>(chunks), work, s);
+  int rc = reserve_frontier(ix, qs, total, s);
+  if (rc) return rc;
+  if ((rc = launch_frontier(ix->forest, descs[0].pred, descs[0].mode, descs, dd, nd,
+                            static_cast<uint32_t>(total), qs.fb, s)))
+    return rc;
+  LaunchPlan fallback = plan;
+  fallback.frontier = false;
+  return launch_queries(ix->forest, fallback, descs, dd, nd, static_cast<uint32_t>(chunks), work, s,
+                        qs.fb.spill, qs.fb.any_spill);
 }
 
 uint64_t sum_queries(const rts_batch* batches, uint32_t n) {
@@ -375,8 +428,7 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   }
   LaunchPlan plan = plan_for(ix, pred, n);
   uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
-  return launch_queries(ix->forest, plan, &b, nullptr, 1, static_cast<uint32_t>(chunks),
-                        static_cast<uint32_t*>(ix->qs.work.ptr), s);
+  return run_launch(ix, ix->qs, plan, &b, nullptr, 1, n, chunks, s);
 }
 
 }  // namespace rts
@@ -581,9 +633,8 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   if (sorted && (rc = fill_order(ix, ix->qs, descs.data(), static_cast<const BatchDesc*>(ddev),
                                  static_cast<uint32_t>(descs.size()), total, s)))
     return rc;
-  return launch_queries(ix->forest, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
-                        static_cast<uint32_t>(descs.size()), static_cast<uint32_t>(chunks),
-                        static_cast<uint32_t*>(ix->qs.work.ptr), s);
+  return run_launch(ix, ix->qs, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
+                    static_cast<uint32_t>(descs.size()), total, chunks, s);
 }
 
 int rts_report_query_time(rts_index* ix, double query_ms, float* rebuild_update_fraction) {

@@ -64,13 +64,13 @@ struct Staging {
 // own QueryScratch.
 struct QueryScratch {
   DevBuf work, keys_a, keys_b, vals, order, sort_temp;
+  // frontier traversal
+  DevBuf fr_qbuf, fr_qaux, fr_qbatch, fr_vis, fr_a, fr_b, fr_counts, fr_spill, fr_any;
+  FrontierBufs fb;
   void release(cudaStream_t s) {
-    buf_free(work, s);
-    buf_free(keys_a, s);
-    buf_free(keys_b, s);
-    buf_free(vals, s);
-    buf_free(order, s);
-    buf_free(sort_temp, s);
+    DevBuf* all[] = {&work, &keys_a, &keys_b, &vals, &order, &sort_temp, &fr_qbuf, &fr_qaux,
+                     &fr_qbatch, &fr_vis, &fr_a, &fr_b, &fr_counts, &fr_spill, &fr_any};
+    for (DevBuf* b : all) buf_free(*b, s);
   }
 };
 
@@ -121,5 +121,14 @@ int fill_order(rts_index* ix, QueryScratch& qs, const BatchDesc* host, const Bat
                uint32_t nd, uint64_t total, cudaStream_t s);
 int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
                const LaunchPlan& plan, std::vector<BatchDesc>& out, uint64_t& chunks);
+// Sizes the frontier buffers of `qs` for `total` queries (no-op when large
+// enough); fills qs.fb.
+int reserve_frontier(rts_index* ix, QueryScratch& qs, uint64_t total, cudaStream_t s);
+// One query launch by the plan's traversal: breadth-first plus its
+// depth-first fallback when the plan asks for it and every batch shares one
+// predicate and handler, depth-first otherwise.  descs: host copies; dd:
+// device copy (required when nd > 1).
+int run_launch(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const BatchDesc* descs,
+               const BatchDesc* dd, uint32_t nd, uint64_t total, uint64_t chunks, cudaStream_t s);
 
 }  // namespace rts

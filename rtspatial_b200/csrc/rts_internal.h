@@ -84,18 +84,44 @@ int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_
 int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
                   float4* leaves, cudaStream_t s);
 
+// ---- frontier traversal (rts_frontier.cu) ---------------------------------
+struct FrontierBufs {
+  void* qbuf = nullptr;       // float4 per query of the launch
+  void* qaux = nullptr;       // float4 per query (range-intersects ray data)
+  uint32_t* qbatch = nullptr; // batch index per query
+  uint32_t* vis = nullptr;    // visiting order: launch index of the i-th query
+  void* fa = nullptr;         // level frontiers (ping-pong), cap entries each
+  void* fb = nullptr;
+  uint32_t cap = 0;
+  uint32_t* counts = nullptr; // frontier sizes, one per level and tree
+  size_t counts_cap = 0;
+  uint32_t* spill = nullptr;  // bitmap of queries answered by the fallback pass
+  uint32_t* any_spill = nullptr;
+};
+// Counters one launch needs (1 + levels of every sub-tree).
+size_t frontier_counts_needed(const Forest& F);
+// Breadth-first pass over every batch (all of one predicate and handler).
+// Queries that overflow the frontier are flagged in fb.spill for a
+// depth-first pass (launch_queries with the same bitmap).
+int launch_frontier(const Forest& F, int pred, int mode, const BatchDesc* hb, const BatchDesc* dd,
+                    uint32_t nb, uint32_t total, const FrontierBufs& fb, cudaStream_t s);
+
 // ---- query launcher (rts_query.cu) ----------------------------------------
 struct LaunchPlan {
   int width = 8;
   bool team = false;
+  bool frontier = false;      // breadth-first pass (plus depth-first fallback)
   uint32_t chunk = 32;  // queries per work item
   bool high_occupancy = false;  // cap registers for 4 CTAs of 256 threads per SM
 };
 // Runs `nb` batches (descriptors in host memory `hb`; device copy `db` when
 // nb > 1) in one persistent launch.  work_counter: zeroed device uint32.
+// only / only_any (nullable): answer just the queries whose launch index
+// (qbase + local) is set in the bitmap, and nothing when *only_any == 0.
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
-                   uint32_t* work_counter, cudaStream_t s);
+                   uint32_t* work_counter, cudaStream_t s, const uint32_t* only = nullptr,
+                   const uint32_t* only_any = nullptr);
 // Number of SMs of the current device (cached).
 int device_sm_count();
 // Resident CTAs per SM of the chosen query kernel (for sizing the grid).

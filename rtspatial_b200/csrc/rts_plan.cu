@@ -44,9 +44,8 @@ int enqueue(rts_plan* p, cudaStream_t s) {
   if (p->sorted && (rc = fill_order(ix, p->qs, p->descs.data(), nd > 1 ? dd : nullptr, nd,
                                     p->total, s)))
     return rc;
-  return launch_queries(ix->forest, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd,
-                        static_cast<uint32_t>(p->chunks), static_cast<uint32_t*>(p->qs.work.ptr),
-                        s);
+  return run_launch(ix, p->qs, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd, p->total,
+                    p->chunks, s);
 }
 
 }  // namespace
@@ -76,6 +75,7 @@ int rts_plan_create(rts_index* ix, const rts_batch* batches, uint32_t n_batches,
     if (!rc) rc = query_order_temp_bytes(p->total, static_cast<uint32_t>(p->descs.size()), &need);
     if (!rc) rc = buf_reserve(p->qs.sort_temp, need, s, false, 0);
   }
+  if (!rc && p->plan.frontier && !p->descs.empty()) rc = reserve_frontier(ix, p->qs, p->total, s);
   if (!rc && !p->descs.empty()) {
     size_t bytes = p->descs.size() * sizeof(BatchDesc);
     rc = buf_reserve(p->ddescs, bytes, s, false, 0);

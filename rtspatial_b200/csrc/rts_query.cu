@@ -13,29 +13,29 @@ namespace rts {
 
 template <int W, bool TEAM, int PRED, int MODE>
 __device__ __forceinline__ void run_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                          uint32_t ce, DevPair* wbuf) {
+                                          uint32_t ce, DevPair* wbuf, const uint32_t* only) {
   if constexpr (TEAM) {
-    run_chunk_team<PRED, MODE, W>(F, B, cb, ce, wbuf);
+    run_chunk_team<PRED, MODE, W>(F, B, cb, ce, wbuf, only);
   } else {
-    run_chunk_thread<PRED, MODE, W>(F, B, cb, ce, wbuf);
+    run_chunk_thread<PRED, MODE, W>(F, B, cb, ce, wbuf, only);
   }
 }
 
 template <int W, bool TEAM>
 __device__ __noinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                            uint32_t ce, DevPair* wbuf) {
+                                            uint32_t ce, DevPair* wbuf, const uint32_t* only) {
   switch (B.pred * 2 + B.mode) {
-    case kPoint * 2 + kCount: run_chunk<W, TEAM, kPoint, kCount>(F, B, cb, ce, wbuf); break;
-    case kPoint * 2 + kCollect: run_chunk<W, TEAM, kPoint, kCollect>(F, B, cb, ce, wbuf); break;
-    case kContains * 2 + kCount: run_chunk<W, TEAM, kContains, kCount>(F, B, cb, ce, wbuf); break;
+    case kPoint * 2 + kCount: run_chunk<W, TEAM, kPoint, kCount>(F, B, cb, ce, wbuf, only); break;
+    case kPoint * 2 + kCollect: run_chunk<W, TEAM, kPoint, kCollect>(F, B, cb, ce, wbuf, only); break;
+    case kContains * 2 + kCount: run_chunk<W, TEAM, kContains, kCount>(F, B, cb, ce, wbuf, only); break;
     case kContains * 2 + kCollect:
-      run_chunk<W, TEAM, kContains, kCollect>(F, B, cb, ce, wbuf);
+      run_chunk<W, TEAM, kContains, kCollect>(F, B, cb, ce, wbuf, only);
       break;
     case kIntersects * 2 + kCount:
-      run_chunk<W, TEAM, kIntersects, kCount>(F, B, cb, ce, wbuf);
+      run_chunk<W, TEAM, kIntersects, kCount>(F, B, cb, ce, wbuf, only);
       break;
     case kIntersects * 2 + kCollect:
-      run_chunk<W, TEAM, kIntersects, kCollect>(F, B, cb, ce, wbuf);
+      run_chunk<W, TEAM, kIntersects, kCollect>(F, B, cb, ce, wbuf, only);
       break;
     default: break;
   }
@@ -47,7 +47,9 @@ template <int W, bool TEAM, int MINB>
 __global__ void __launch_bounds__(kQueryThreads, MINB)
     k_query(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
             const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
-            uint32_t chunk, uint32_t* __restrict__ work) {
+            uint32_t chunk, uint32_t* __restrict__ work, const uint32_t* __restrict__ only,
+            const uint32_t* __restrict__ only_any) {
+  if (only_any && *only_any == 0) return;
   __shared__ Forest F;
   __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
   {
@@ -75,12 +77,12 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     }
     const uint32_t cb = (c - B.chunk_begin) * chunk;
     const uint32_t ce = min(cb + chunk, B.n);
-    dispatch_chunk<W, TEAM>(F, B, cb, ce, wbufs[threadIdx.x / 32]);
+    dispatch_chunk<W, TEAM>(F, B, cb, ce, wbufs[threadIdx.x / 32], only);
   }
 }
 
 using QueryKernel = void (*)(const Forest, const BatchDesc, const BatchDesc*, uint32_t, uint32_t,
-                             uint32_t, uint32_t*);
+                             uint32_t, uint32_t*, const uint32_t*, const uint32_t*);
 
 template <int MINB>
 static QueryKernel pick_kernel_occ(const LaunchPlan& p) {
@@ -133,13 +135,15 @@ int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks) {
 
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
-                   uint32_t* work_counter, cudaStream_t s) {
+                   uint32_t* work_counter, cudaStream_t s, const uint32_t* only,
+                   const uint32_t* only_any) {
   if (total_chunks == 0) return RTS_OK;
   QueryKernel k = pick_kernel(plan);
   if (!k) return fail(RTS_ERR_INVALID_ARGUMENT, "unsupported node width / traversal");
   int grid = query_grid_size(plan, total_chunks);
   RTS_CUDA_TRY(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), s));
-  k<<<grid, kQueryThreads, 0, s>>>(F, hb[0], db, nb, total_chunks, plan.chunk, work_counter);
+  k<<<grid, kQueryThreads, 0, s>>>(F, hb[0], db, nb, total_chunks, plan.chunk, work_counter, only,
+                                   only_any);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }

@@ -52,8 +52,12 @@ struct TravState {
 // Returns false when the forest is empty.
 template <int PRED, int W>
 __device__ __forceinline__ bool trav_start(const Forest& F, const BatchDesc& B, uint32_t slot,
-                                           TravState<PRED, W>& s) {
+                                           TravState<PRED, W>& s, const uint32_t* only) {
   s.qid = B.order ? B.order[slot] : slot;
+  if (only) {
+    const uint32_t g = B.qbase + s.qid;
+    if (!((__ldg(only + (g >> 5)) >> (g & 31)) & 1u)) return false;
+  }
   s.q = QueryOps<PRED>::load(B.queries, s.qid);
   s.ms.clear();
   s.t = 0;
@@ -101,7 +105,8 @@ __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>
 // ---------------------------------------------------------------------------
 template <int PRED, int MODE, int W>
 __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDesc& B,
-                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf) {
+                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf,
+                                                 const uint32_t* only) {
   using Ops = QueryOps<PRED>;
   const uint32_t lane = lane_id();
   TravState<PRED, W> s;
@@ -109,7 +114,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
   bool active = false;
   {
     uint32_t slot = next + lane;
-    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
     next = min(cend, next + 32u);
   }
   DevQueue qu{};
@@ -156,7 +161,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
     uint32_t idle = __ballot_sync(kFull, !active);
     if (idle != 0 && next < cend) {
       uint32_t slot = next + __popc(idle & lanemask_lt());
-      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
       next = min(cend, next + __popc(idle));
     }
   }
@@ -169,7 +174,8 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
 // ---------------------------------------------------------------------------
 template <int PRED, int MODE, int W>
 __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc& B,
-                                               uint32_t cbeg, uint32_t cend, DevPair* wbuf) {
+                                               uint32_t cbeg, uint32_t cend, DevPair* wbuf,
+                                               const uint32_t* only) {
   using Ops = QueryOps<PRED>;
   constexpr uint32_t kTeams = 32 / W;
   constexpr uint32_t kTeamMask = (W == 32) ? kFull : ((1u << W) - 1u);
@@ -181,7 +187,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
   bool active = false;
   {
     uint32_t slot = next + team;
-    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
     next = min(cend, next + kTeams);
   }
   DevQueue qu{};
@@ -220,7 +226,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
     if (idle != 0 && next < cend) {
       uint32_t below = (team == 0) ? 0u : (idle & ((1u << (team * W)) - 1u));
       uint32_t slot = next + __popc(below) / W;
-      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s);
+      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
       next = min(cend, next + __popc(idle) / W);
     }
   }

@@ -135,6 +135,7 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
       {RTS_TRAVERSAL_THREAD, 0, 1, 32},   {RTS_TRAVERSAL_THREAD, 0, 1, 128},
       {RTS_TRAVERSAL_THREAD, 4, 1, 64},   {RTS_TRAVERSAL_THREAD, 4, 1, 128},
       {RTS_TRAVERSAL_TEAM, 0, 1, 64},     {RTS_TRAVERSAL_TEAM, 4, 1, 128},
+      {RTS_TRAVERSAL_FRONTIER, 4, 0, 64}, {RTS_TRAVERSAL_FRONTIER, 4, 1, 64},
   };
   double best = 1e300, first = -1;
   int best_w = ix->W;

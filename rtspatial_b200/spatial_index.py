@@ -80,6 +80,7 @@ class Config:
     rebuild_update_fraction: float = 0.25
     chunk: int = 0
     query_occupancy: int = 0
+    frontier_factor: float = 0.0
 
     def to_c(self) -> L.rts_config:
         c = L.rts_config()

@@ -11,7 +11,7 @@ import rtspatial_b200 as rb
 from rtspatial_b200 import _lib as L
 
 WIDTHS = (4, 8, 16, 32)
-TRAVERSALS = (L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_TEAM)
+TRAVERSALS = (L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_TEAM, L.RTS_TRAVERSAL_FRONTIER)
 CURVES = (L.RTS_CURVE_MORTON, L.RTS_CURVE_HILBERT)
 
 # every (width, traversal, curve) combination
@@ -23,7 +23,9 @@ SOME_COMBOS = [(w, t, CURVES[i % 2]) for i, (w, t) in
 
 def combo_id(c):
     w, t, cu = c
-    return f"w{w}-{'thread' if t == L.RTS_TRAVERSAL_THREAD else 'team'}-" \
+    tn = {L.RTS_TRAVERSAL_THREAD: "thread", L.RTS_TRAVERSAL_TEAM: "team",
+          L.RTS_TRAVERSAL_FRONTIER: "frontier"}[t]
+    return f"w{w}-{tn}-" \
            f"{'morton' if cu == L.RTS_CURVE_MORTON else 'hilbert'}"
 
 

@@ -174,3 +174,27 @@ def test_batched_count_handlers(cuda, workloads):
     torch.cuda.synchronize()
     assert [c.get() for c in cs] == [want["point"].shape[0], want["contains"].shape[0],
                                      want["intersects"].shape[0]]
+
+
+@pytest.mark.parametrize("w", [4, 8, 16, 32])
+@pytest.mark.parametrize("factor", [0.05, 1.0], ids=["spill", "fits"])
+def test_frontier_spill_falls_back_exactly(cuda, workloads, w, factor):
+    # A frontier too small for the launch flags the overflowing queries; the
+    # depth-first pass answers exactly those, so no pair is lost or doubled.
+    b, p, q, want = workloads["clustered"]
+    ix = rb.SpatialIndex(rb.Config(node_width=w, traversal=rb._lib.RTS_TRAVERSAL_FRONTIER,
+                                   frontier_factor=factor, max_trees=4, rebuild_fraction=1e9))
+    for part in np.array_split(b, 3):
+        ix.Insert(dev(part))
+    assert ix.num_trees() == 3
+    assert_same_pairs(gpu_pairs(ix, P.kContains, p), want["point"], "point")
+    assert_same_pairs(gpu_pairs(ix, P.kContains, q), want["contains"], "contains")
+    assert_same_pairs(gpu_pairs(ix, P.kIntersects, q), want["intersects"], "intersects")
+    # batched, several batches of one predicate
+    queues = [rb.Queue(400_000) for _ in range(4)]
+    parts = np.array_split(q, 4)
+    ix.query_batched([(P.kIntersects, dev(a), rb.Handler.COLLECT, qu.DeviceObject())
+                      for a, qu in zip(parts, queues)])
+    torch.cuda.synchronize()
+    for a, qu in zip(parts, queues):
+        assert_same_pairs(canon(qu.result()), oracle_pairs("intersects", b, a), "batched")
