@@ -652,17 +652,24 @@ def run_serving_bench(args, ctx):
                     update_boxes=wl.uniform_boxes(rng, k, 1e-3),
                     inserts=wl.uniform_boxes(rng, k, 1e-3))
 
-    sv = rb.Server(ix, slots=3, max_queries_per_launch=1 << 19, pairs_per_launch=16 << 20)
+    sv = rb.Server(ix, slots=3, max_queries_per_launch=1 << 19, pairs_per_launch=16 << 20,
+                   host_result_bytes=4 << 30)
+    # the client's result buffer, reused for every request (touched once here)
+    out_buf = np.ones((64 << 20, 2), dtype=np.uint32)
+
+    def take(t):
+        return sv.take(t, out=out_buf)
+
     # closed loop: everything submitted at once -> capacity
     warm = make_requests(20)
     for t in [sv.submit(p, q) for p, q in warm]:
-        sv.take(t)
+        take(t)
     reqs = make_requests(n_req)
     sv.reset_stats()
     t0 = time.perf_counter()
     tickets = [sv.submit(p, q) for p, q in reqs]
     for t in tickets:
-        sv.take(t)
+        take(t)
     closed_s = time.perf_counter() - t0
     closed = sv.stats()
     total_q = sum(q.shape[0] for _, q in reqs)
@@ -690,7 +697,7 @@ def run_serving_bench(args, ctx):
         if i % 10 == 9 and ups:
             up_tickets.append(sv.submit_update(**ups.pop()))
     for t in tickets:
-        sv.take(t)
+        take(t)
     for t in up_tickets:
         sv.take(t)
     open_s = time.perf_counter() - t0

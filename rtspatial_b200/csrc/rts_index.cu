@@ -471,7 +471,8 @@ int rts_create(const rts_config* cfg, rts_index** out) {
   if (cfg) c = *cfg; else rts_config_default(&c);
   if (c.node_width != 4 && c.node_width != 8 && c.node_width != 16 && c.node_width != 32)
     return fail(RTS_ERR_INVALID_ARGUMENT, "node_width must be 4, 8, 16 or 32");
-  if (c.traversal < 0 || c.traversal > 2) return fail(RTS_ERR_INVALID_ARGUMENT, "bad traversal");
+  if (c.traversal < 0 || c.traversal > RTS_TRAVERSAL_FRONTIER)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "bad traversal");
   if (c.curve != RTS_CURVE_MORTON && c.curve != RTS_CURVE_HILBERT)
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad curve");
   if (c.max_trees < 1 || c.max_trees > kMaxTrees)

@@ -83,6 +83,16 @@ def test_argument_validation_without_gpu():
     c.max_trees = 0
     assert lib.rts_create(ctypes.byref(c), ctypes.byref(h)) == L.RTS_ERR_INVALID_ARGUMENT
     c.max_trees = 8
+    # every traversal scheme the header defines is accepted at creation
+    for t in (L.RTS_TRAVERSAL_AUTO, L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_TEAM,
+              L.RTS_TRAVERSAL_FRONTIER):
+        c.traversal = t
+        h2 = ctypes.c_void_p()
+        assert lib.rts_create(ctypes.byref(c), ctypes.byref(h2)) == L.RTS_OK, t
+        lib.rts_destroy(h2)
+    c.traversal = 9
+    assert lib.rts_create(ctypes.byref(c), ctypes.byref(h)) == L.RTS_ERR_INVALID_ARGUMENT
+    c.traversal = L.RTS_TRAVERSAL_AUTO
     assert lib.rts_create(ctypes.byref(c), ctypes.byref(h)) == L.RTS_OK
     try:
         assert lib.rts_size(h) == 0 and lib.rts_num_trees(h) == 0
