@@ -122,7 +122,16 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
   WarpOut out{wbuf, 0};
   unsigned long long cnt = 0;
 
-  while (__any_sync(kFull, active)) {
+  for (;;) {
+    if (!__any_sync(kFull, active)) {
+      // Every lane is idle (with a query filter, refills can all be rejected):
+      // refill again until the chunk is exhausted.
+      if (next >= cend) break;
+      uint32_t slot = next + lane;
+      if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+      next = min(cend, next + 32u);
+      continue;
+    }
     uint32_t leafm = 0;
     const uint32_t* leafids = nullptr;
     if (active) {
@@ -195,7 +204,14 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
   WarpOut out{wbuf, 0};
   unsigned long long cnt = 0;
 
-  while (__any_sync(kFull, active)) {
+  for (;;) {
+    if (!__any_sync(kFull, active)) {
+      if (next >= cend) break;  // see run_chunk_thread
+      uint32_t slot = next + team;
+      if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+      next = min(cend, next + kTeams);
+      continue;
+    }
     bool hit = false, leaf_hit = false;
     uint32_t gid = 0;
     if (active) {

@@ -177,7 +177,8 @@ def test_batched_count_handlers(cuda, workloads):
 
 
 @pytest.mark.parametrize("w", [4, 8, 16, 32])
-@pytest.mark.parametrize("factor", [0.05, 1.0], ids=["spill", "fits"])
+@pytest.mark.parametrize("factor", [0.05, 0.5, 2.0, 64.0],
+                         ids=["spill-most", "spill-many", "spill-some", "fits"])
 def test_frontier_spill_falls_back_exactly(cuda, workloads, w, factor):
     # A frontier too small for the launch flags the overflowing queries; the
     # depth-first pass answers exactly those, so no pair is lost or doubled.
