@@ -37,9 +37,9 @@ struct TreeDesc {
 
 struct Forest {
   TreeDesc tree[kMaxTrees];
+  const uint32_t* ids_base;  // leaf_ids of slot 0 (all sub-trees share the array)
   uint32_t n_trees;
   uint32_t width;
-  uint32_t pad[2];
 };
 
 // Collecting handler target: member layout of
@@ -299,14 +299,18 @@ __device__ __forceinline__ void collect_warp(const DevQueue& qu, uint32_t m,
 }
 
 // Warp-private staging of collected pairs in shared memory.  Pairs found in a
-// step are written to the warp's buffer; the buffer is flushed to the queue
-// with one atomicAdd and coalesced 8-byte stores when it would overflow and
-// when the warp finishes its chunk.  All calls are made by all 32 lanes.
+// step are written to the warp's buffer as (leaf slot, query id); the buffer
+// is flushed to the queue with one atomicAdd and coalesced 8-byte stores when
+// it would overflow and when the warp finishes its chunk.  The flush turns
+// slots into ids: those loads are independent, so they overlap once per flush
+// instead of adding a dependent load to the query's path at every leaf.  All
+// calls are made by all 32 lanes.
 constexpr uint32_t kWarpOutCap = 256;
 
 struct WarpOut {
-  DevPair* buf;   // kWarpOutCap entries in shared memory, private to the warp
-  uint32_t n;     // pairs buffered (same value in every lane)
+  DevPair* buf;          // kWarpOutCap entries in shared memory, private to the warp
+  uint32_t n;            // pairs buffered (same value in every lane)
+  const uint32_t* ids;   // leaf_ids of slot 0
 
   __device__ __forceinline__ void flush(const DevQueue& qu) {
     if (n == 0) return;
@@ -315,18 +319,17 @@ struct WarpOut {
     if (lane_id() == 0) base = atomicAdd(qu.size, n);
     base = __shfl_sync(kFull, base, 0);
     for (uint32_t i = lane_id(); i < n; i += 32) {
+      const DevPair e = buf[i];
       unsigned long long p = static_cast<unsigned long long>(base) + i;
-      if (p < qu.capacity) qu.data[p] = buf[i];
+      if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + e.geom_id), e.query_id};
     }
     __syncwarp();
     n = 0;
   }
 
-  // Adds, for every lane, (ids[c], qid) for each set bit c of m (c < W).
-  // The id loads are unrolled and predicated so they are all in flight at
-  // once instead of one dependent load per pair.
+  // Adds, for every lane, (slot0 + c, qid) for each set bit c of m (c < W).
   template <int W>
-  __device__ __forceinline__ void add(const DevQueue& qu, uint32_t m, const uint32_t* ids,
+  __device__ __forceinline__ void add(const DevQueue& qu, uint32_t m, uint32_t slot0,
                                       uint32_t qid) {
     if (!__any_sync(kFull, m != 0)) return;
     const uint32_t lane = lane_id();
@@ -348,7 +351,7 @@ struct WarpOut {
       for (int c = 0; c < W; ++c) {
         if ((m >> c) & 1u) {
           unsigned long long p = p0 + __popc(m & ((1u << c) - 1u));
-          if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + c), qid};
+          if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + slot0 + c), qid};
         }
       }
       return;
@@ -356,18 +359,18 @@ struct WarpOut {
     const uint32_t at = n + incl - cnt;
 #pragma unroll
     for (int c = 0; c < W; ++c)
-      if ((m >> c) & 1u) buf[at + __popc(m & ((1u << c) - 1u))] = DevPair{__ldg(ids + c), qid};
+      if ((m >> c) & 1u) buf[at + __popc(m & ((1u << c) - 1u))] = DevPair{slot0 + c, qid};
     n += total;
   }
 
-  // Team scheme: each lane has at most one pair.
-  __device__ __forceinline__ void add_one(const DevQueue& qu, bool hit, uint32_t gid,
+  // Team scheme: each lane has at most one pair (its leaf slot).
+  __device__ __forceinline__ void add_one(const DevQueue& qu, bool hit, uint32_t slot,
                                           uint32_t qid) {
     const uint32_t bal = __ballot_sync(kFull, hit);
     if (bal == 0) return;
     const uint32_t total = __popc(bal);
     if (n + total > kWarpOutCap) flush(qu);
-    if (hit) buf[n + __popc(bal & ((1u << lane_id()) - 1u))] = DevPair{gid, qid};
+    if (hit) buf[n + __popc(bal & ((1u << lane_id()) - 1u))] = DevPair{slot, qid};
     n += total;
   }
 };

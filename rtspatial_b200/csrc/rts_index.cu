@@ -227,6 +227,7 @@ void refresh_forest(rts_index* ix) {
   std::memset(&F, 0, sizeof(F));
   F.n_trees = static_cast<uint32_t>(ix->trees.size());
   F.width = static_cast<uint32_t>(ix->W);
+  F.ids_base = ids_of(ix);
   for (size_t i = 0; i < ix->trees.size(); ++i) {
     const HostTree& h = ix->trees[i];
     TreeDesc& d = F.tree[i];

@@ -119,7 +119,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
   }
   DevQueue qu{};
   if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
-  WarpOut out{wbuf, 0};
+  WarpOut out{wbuf, 0, F.ids_base};
   unsigned long long cnt = 0;
 
   for (;;) {
@@ -133,7 +133,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       continue;
     }
     uint32_t leafm = 0;
-    const uint32_t* leafids = nullptr;
+    uint32_t leafslot = 0;
     if (active) {
       // One load-and-test path for leaves and nodes (no divergent copies).
       const TreeDesc& T = F.tree[s.t];
@@ -155,13 +155,13 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
             if (((m >> c) & 1u) && !Ops::exact(e[c], s.q)) m &= ~(1u << c);
         }
         leafm = m;
-        leafids = T.ids + first;
+        leafslot = static_cast<uint32_t>(T.ids - F.ids_base) + first;
       } else {
         s.ms.set(s.L, m);
       }
     }
     if (MODE == kCollect) {
-      out.template add<W>(qu, leafm, leafids, s.qid + B.id_offset);
+      out.template add<W>(qu, leafm, leafslot, s.qid + B.id_offset);
     } else {
       cnt += __popc(leafm);
     }
@@ -201,7 +201,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
   }
   DevQueue qu{};
   if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
-  WarpOut out{wbuf, 0};
+  WarpOut out{wbuf, 0, F.ids_base};
   unsigned long long cnt = 0;
 
   for (;;) {
@@ -221,7 +221,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
         float4 e = __ldg(T.leaves + first + tl);
         hit = (first + tl < T.n) && Ops::leaf(e, s.q);
         leaf_hit = hit;
-        if (leaf_hit) gid = __ldg(T.ids + first + tl);
+        if (leaf_hit) gid = static_cast<uint32_t>(T.ids - F.ids_base) + first + tl;
       } else {
         float4 e = __ldg(T.nodes + T.level_off[s.L] + first + tl);
         hit = (first + tl < T.level_cnt[s.L]) && Ops::node(e, s.q);
