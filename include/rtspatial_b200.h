@@ -112,7 +112,8 @@ typedef struct rts_config {
   float rebuild_update_fraction; /* updates since the last rebuild, as a fraction of the index,
                                     above which Update re-sorts instead of refitting */
   uint32_t chunk;         /* queries per device work item (0 = library default) */
-  int32_t query_occupancy; /* 0 library default; 4: query kernel capped at 64 registers */
+  int32_t query_occupancy; /* 0 library default; 2 / 4: query kernel capped at 128 / 64
+                              registers (2 / 4 CTAs of 256 threads per SM) */
   float frontier_factor;   /* frontier traversal: entries per query of each level buffer
                               (queries beyond it are answered depth-first); 0 = 16 */
 } rts_config;
@@ -122,6 +123,8 @@ typedef struct rts_config {
 #define RTS_TRAVERSAL_TEAM 2   /* node_width lanes per query, one child per lane */
 #define RTS_TRAVERSAL_FRONTIER 3 /* level by level over the whole launch (batches of one
                                     predicate and handler; others run depth-first) */
+#define RTS_TRAVERSAL_PACKET 4 /* one warp walks a packet of up to 32 queries, one entry
+                                  per lane; best with sorted queries */
 
 #define RTS_CURVE_MORTON 0
 #define RTS_CURVE_HILBERT 1
@@ -171,7 +174,11 @@ int rts_query_envelopes(rts_index* index, int predicate, const float* envelopes,
 /* ---- batched queries ----------------------------------------------------
  * Many Query calls fused into one persistent launch with a device-side work
  * queue.  Each batch keeps its own handler/arg and its own 0-based query ids,
- * so a batch's results equal those of the same Query call made alone. */
+ * so a batch's results equal those of the same Query call made alone.  When
+ * the launch sorts its queries, every batch has one predicate and handler,
+ * and the handler counts or the traversal is RTS_TRAVERSAL_PACKET, the
+ * queries of all batches are sorted together and each result is routed to its
+ * batch's handler. */
 #define RTS_QUERY_POINTS 0
 #define RTS_QUERY_ENVELOPES 1
 typedef struct rts_batch {

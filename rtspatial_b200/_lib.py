@@ -29,6 +29,7 @@ RTS_TRAVERSAL_AUTO = 0
 RTS_TRAVERSAL_THREAD = 1
 RTS_TRAVERSAL_TEAM = 2
 RTS_TRAVERSAL_FRONTIER = 3
+RTS_TRAVERSAL_PACKET = 4
 RTS_CURVE_MORTON = 0
 RTS_CURVE_HILBERT = 1
 RTS_QUERY_POINTS = 0

@@ -7,6 +7,7 @@ products.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -46,14 +47,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compiles the shared library if any source is newer; returns its path."""
     if not force and not _stale():
         return LIB
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(CSRC, "_" + src.replace(".cu", ".o"))
         cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.check_call(cmd)
+        cmds.append(cmd)
         objs.append(obj)
+    # one nvcc per source, in parallel (the query kernels dominate)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     subprocess.check_call([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
                            *objs, "-o", tmp])

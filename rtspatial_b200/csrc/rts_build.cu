@@ -182,24 +182,30 @@ __global__ void k_update(const rts_update_entry* __restrict__ upd, uint64_t n, u
   leaves[pos[e.id]] = make_float4(e.min_x, e.min_y, e.max_x, e.max_y);
 }
 
+__device__ __forceinline__ uint32_t batch_of_query(const BatchDesc* descs, uint32_t nb,
+                                                   uint64_t i) {
+  if (nb <= 1) return 0;
+  uint32_t lo = 0, hi = nb - 1;  // largest b with qbase <= i
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (descs[mid].qbase <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Visiting order of queries: key = (batch index << 32) | curve index of the
 // query's centre in the frame of the first sub-tree's root box; value = the
 // query's index within its batch.  Sorting by key groups batches and, within
-// a batch, puts queries that walk the same nodes next to each other.
+// a batch, puts queries that walk the same nodes next to each other.  Merged:
+// key = curve index alone, value = the query's index in the launch, so the
+// sort interleaves the batches by position.
 __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDesc b0, uint32_t nb,
                              uint64_t total, const float4* __restrict__ frame_box, int curve,
-                             unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals) {
+                             unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals,
+                             bool merged) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
-  uint32_t b = 0;
-  if (nb > 1) {
-    uint32_t lo = 0, hi = nb - 1;  // largest b with qbase <= i
-    while (lo < hi) {
-      uint32_t mid = (lo + hi + 1) >> 1;
-      if (descs[mid].qbase <= i) lo = mid; else hi = mid - 1;
-    }
-    b = lo;
-  }
+  const uint32_t b = batch_of_query(descs, nb, i);
   const BatchDesc& B = (nb > 1) ? descs[b] : b0;
   const uint32_t local = static_cast<uint32_t>(i - B.qbase);
   float2 c;
@@ -214,8 +220,31 @@ __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDes
   uint32_t qx = __float2uint_rz(fminf(fmaxf((c.x - f.x) * sx, 0.0f), 65535.0f));
   uint32_t qy = __float2uint_rz(fminf(fmaxf((c.y - f.y) * sy, 0.0f), 65535.0f));
   uint32_t k = (curve == RTS_CURVE_HILBERT) ? hilbert16(qx, qy) : (spread16(qx) | (spread16(qy) << 1));
-  keys[i] = (static_cast<unsigned long long>(b) << 32) | k;
-  vals[i] = local;
+  keys[i] = merged ? k : (static_cast<unsigned long long>(b) << 32) | k;
+  vals[i] = merged ? static_cast<uint32_t>(i) : local;
+}
+
+// Merged launch: copies the queries in sorted order (order[j] = index in the
+// launch) and records each position's batch and reported query id.  The
+// first nb threads also copy the batches' queue headers into routes.
+__global__ void k_merge_queries(const BatchDesc* __restrict__ descs, uint32_t nb, uint64_t total,
+                                const uint32_t* __restrict__ order, void* __restrict__ out_q,
+                                uint32_t* __restrict__ out_batch, uint32_t* __restrict__ out_ident,
+                                DevQueue* __restrict__ routes) {
+  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (routes && j < nb) routes[j] = *static_cast<const DevQueue*>(descs[j].arg);
+  if (j >= total) return;
+  const uint32_t g = order[j];
+  const uint32_t b = batch_of_query(descs, nb, g);
+  const BatchDesc& B = descs[b];
+  const uint32_t local = g - B.qbase;
+  if (B.pred == kPoint) {
+    reinterpret_cast<float2*>(out_q)[j] = reinterpret_cast<const float2*>(B.queries)[local];
+  } else {
+    reinterpret_cast<float4*>(out_q)[j] = reinterpret_cast<const float4*>(B.queries)[local];
+  }
+  out_batch[j] = b;
+  out_ident[j] = local + B.id_offset;
 }
 
 inline unsigned grid_for(uint64_t n) {
@@ -327,13 +356,15 @@ int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint
 int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
                        const float4* frame_box, int curve, unsigned long long* keys_a,
                        unsigned long long* keys_b, uint32_t* vals_a, uint32_t* order,
-                       DevBuf& temp, cudaStream_t s) {
+                       DevBuf& temp, cudaStream_t s, bool merged, void* merged_q,
+                       uint32_t* merged_batch, uint32_t* merged_ident, DevQueue* merged_routes) {
   if (total == 0) return RTS_OK;
+  merged = merged && nb > 1;
   k_query_keys<<<grid_for(total), kThreads, 0, s>>>(descs, b0, nb, total, frame_box, curve, keys_a,
-                                                    vals_a);
+                                                    vals_a, merged);
   RTS_CUDA_TRY(cudaGetLastError());
   int end_bit = 32;
-  while (end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
+  while (!merged && end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
   size_t need = 0;
   RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, keys_a, keys_b, vals_a, order,
                                                 static_cast<int>(total), 0, end_bit, s));
@@ -341,6 +372,13 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
   if (rc) return rc;
   RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.ptr, need, keys_a, keys_b, vals_a, order,
                                                 static_cast<int>(total), 0, end_bit, s));
+  if (merged) {
+    // nb <= total: every batch of a merged launch is non-empty
+    k_merge_queries<<<grid_for(total), kThreads, 0, s>>>(descs, nb, total, order, merged_q,
+                                                         merged_batch, merged_ident,
+                                                         merged_routes);
+    RTS_CUDA_TRY(cudaGetLastError());
+  }
   return RTS_OK;
 }
 

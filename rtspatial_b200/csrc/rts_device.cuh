@@ -298,6 +298,44 @@ __device__ __forceinline__ void collect_warp(const DevQueue& qu, uint32_t m,
   }
 }
 
+// Parameters of one batch (one reference Query call).
+struct BatchDesc {
+  const float* queries;
+  void* arg;              // counter (count) or DevQueue* (collect)
+  uint32_t n;             // queries in the batch
+  int32_t pred;           // PredKind
+  int32_t mode;           // HandlerKind
+  uint32_t chunk_begin;   // index of the batch's first chunk in the launch
+  const uint32_t* order;  // optional visiting order (query ids), or nullptr
+  uint32_t qbase;         // offset of the batch in the launch's concatenated order
+  uint32_t id_offset;     // added to every reported query id (0 for a Query call)
+};
+
+// Launch-wide visiting order.  When every batch of a launch shares one
+// predicate and handler, the queries of all batches are sorted together and
+// copied into one array, which the kernel runs as a single batch; results are
+// routed back per query.  batch == nullptr: the launch runs batch by batch.
+struct MergedOrder {
+  const BatchDesc* descs;  // the launch's batches (device copy)
+  const uint32_t* batch;   // sorted position -> batch index
+  const uint32_t* ident;   // sorted position -> query id reported to that batch
+  const DevQueue* routes;  // collect: copy of each batch's queue header, by batch index
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Counting handler of a merged launch: adds one finished query's count to
+// its batch (b) counter.
+__device__ __forceinline__ void count_routed(const MergedOrder& mo, uint32_t b,
+                                             unsigned long long c) {
+  if (c == 0) return;
+  atomicAdd(static_cast<unsigned long long*>(mo.descs[b].arg), c);
+}
+
 // Warp-private staging of collected pairs in shared memory.  Pairs found in a
 // step are written to the warp's buffer as (leaf slot, query id); the buffer
 // is flushed to the queue with one atomicAdd and coalesced 8-byte stores when
@@ -306,31 +344,106 @@ __device__ __forceinline__ void collect_warp(const DevQueue& qu, uint32_t m,
 // instead of adding a dependent load to the query's path at every leaf.  All
 // calls are made by all 32 lanes.
 constexpr uint32_t kWarpOutCap = 256;
+// Batch table of a merged launch's flush (per warp, after the batch indices).
+constexpr uint32_t kRouteBits = 6;
+constexpr uint32_t kRouteSlots = 1u << kRouteBits;
+constexpr uint32_t kWarpBatWords = kWarpOutCap + 3 * kRouteSlots;
 
+template <bool ROUTED>
 struct WarpOut {
-  DevPair* buf;          // kWarpOutCap entries in shared memory, private to the warp
-  uint32_t n;            // pairs buffered (same value in every lane)
-  const uint32_t* ids;   // leaf_ids of slot 0
+  DevPair* buf;              // kWarpOutCap entries in shared memory, private to the warp
+  uint32_t* bat;             // merged launch: batch index of each entry, then the
+                             // flush's batch table (kWarpBatWords, shared memory)
+  uint32_t n;                // pairs buffered (same value in every lane)
+  const uint32_t* ids;       // leaf_ids of slot 0
+  // Routing of a merged launch (ROUTED), kept in registers.
+  const uint32_t* ident;
+  const DevQueue* routes;
+
+  __device__ __forceinline__ WarpOut(DevPair* b, uint32_t* bt, const uint32_t* leaf_ids,
+                                     const MergedOrder& mo)
+      : buf(b), bat(bt), n(0), ids(leaf_ids), ident(mo.ident),
+        routes(mo.routes) {}
 
   __device__ __forceinline__ void flush(const DevQueue& qu) {
     if (n == 0) return;
     __syncwarp();
-    uint32_t base = 0;
-    if (lane_id() == 0) base = atomicAdd(qu.size, n);
-    base = __shfl_sync(kFull, base, 0);
-    for (uint32_t i = lane_id(); i < n; i += 32) {
-      const DevPair e = buf[i];
-      unsigned long long p = static_cast<unsigned long long>(base) + i;
-      if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + e.geom_id), e.query_id};
+    if constexpr (ROUTED) {
+      flush_routed();
+    } else {
+      uint32_t base = 0;
+      if (lane_id() == 0) base = atomicAdd(qu.size, n);
+      base = __shfl_sync(kFull, base, 0);
+      for (uint32_t i = lane_id(); i < n; i += 32) {
+        const DevPair e = buf[i];
+        unsigned long long p = static_cast<unsigned long long>(base) + i;
+        if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + e.geom_id), e.query_id};
+      }
     }
     __syncwarp();
     n = 0;
   }
 
-  // Adds, for every lane, (slot0 + c, qid) for each set bit c of m (c < W).
+  // Merged launch: buffered query ids are sorted positions, bat[] their
+  // batches.  The buffer is grouped by batch in a small hash table in shared
+  // memory (tab, kRouteSlots keys + counts + bases): each entry takes a rank
+  // within its batch with a shared-memory atomic, then one global atomicAdd
+  // per distinct batch reserves that batch's slots — all of them issued at
+  // once — and every entry writes to base + rank.  Entries whose batch finds
+  // no free table slot reserve their own slot directly.
+  __device__ __forceinline__ void flush_routed() {
+    constexpr uint32_t kEmpty = 0xffffffffu;
+    const uint32_t lane = lane_id();
+    uint32_t* keys = bat + kWarpOutCap;
+    uint32_t* cnts = keys + kRouteSlots;
+    uint32_t* bases = cnts + kRouteSlots;
+    for (uint32_t k = lane; k < kRouteSlots; k += 32) {
+      keys[k] = kEmpty;
+      cnts[k] = 0;
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) {
+      const uint32_t b = bat[i];
+      const uint32_t h = (b * 0x9E3779B1u) >> (32 - kRouteBits);
+      uint32_t slot = kRouteSlots;
+      for (uint32_t probe = 0; probe < kRouteSlots; ++probe) {
+        const uint32_t k = (h + probe) & (kRouteSlots - 1);
+        const uint32_t prev = atomicCAS(&keys[k], kEmpty, b);
+        if (prev == kEmpty || prev == b) {
+          slot = k;
+          break;
+        }
+      }
+      if (slot < kRouteSlots) {
+        bat[i] = (slot << 16) | atomicAdd(&cnts[slot], 1u);
+      } else {  // table full: this entry reserves its own slot
+        const DevPair e = buf[i];
+        const DevQueue Q = routes[b];
+        const unsigned long long p = atomicAdd(Q.size, 1u);
+        if (p < Q.capacity) Q.data[p] = DevPair{__ldg(ids + e.geom_id), __ldg(ident + e.query_id)};
+        bat[i] = kEmpty;
+      }
+    }
+    __syncwarp();
+    for (uint32_t k = lane; k < kRouteSlots; k += 32)
+      if (cnts[k]) bases[k] = atomicAdd(routes[keys[k]].size, cnts[k]);
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) {
+      const uint32_t v = bat[i];
+      if (v == kEmpty) continue;
+      const DevPair e = buf[i];
+      const uint32_t slot = v >> 16;
+      const DevQueue Q = routes[keys[slot]];
+      const unsigned long long p = static_cast<unsigned long long>(bases[slot]) + (v & 0xffffu);
+      if (p < Q.capacity) Q.data[p] = DevPair{__ldg(ids + e.geom_id), __ldg(ident + e.query_id)};
+    }
+  }
+
+  // Adds, for every lane, (slot0 + c, qid) for each set bit c of m (c < W);
+  // rb = the query's batch in a merged launch.
   template <int W>
   __device__ __forceinline__ void add(const DevQueue& qu, uint32_t m, uint32_t slot0,
-                                      uint32_t qid) {
+                                      uint32_t qid, uint32_t rb) {
     if (!__any_sync(kFull, m != 0)) return;
     const uint32_t lane = lane_id();
     uint32_t cnt = __popc(m);
@@ -342,6 +455,21 @@ struct WarpOut {
     }
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     if (n + total > kWarpOutCap) flush(qu);
+    if (ROUTED && total > kWarpOutCap) {  // more than a buffer, merged launch
+      if (cnt) {
+        const DevQueue Q = routes[rb];
+        const uint32_t rid = __ldg(ident + qid);
+        const unsigned long long p0 = atomicAdd(Q.size, cnt);
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+          if ((m >> c) & 1u) {
+            unsigned long long p = p0 + __popc(m & ((1u << c) - 1u));
+            if (p < Q.capacity) Q.data[p] = DevPair{__ldg(ids + slot0 + c), rid};
+          }
+        }
+      }
+      return;
+    }
     if (total > kWarpOutCap) {  // more than a buffer: straight to the queue
       uint32_t base = 0;
       if (lane == 31) base = atomicAdd(qu.size, total);
@@ -358,19 +486,76 @@ struct WarpOut {
     }
     const uint32_t at = n + incl - cnt;
 #pragma unroll
-    for (int c = 0; c < W; ++c)
-      if ((m >> c) & 1u) buf[at + __popc(m & ((1u << c) - 1u))] = DevPair{slot0 + c, qid};
+    for (int c = 0; c < W; ++c) {
+      if ((m >> c) & 1u) {
+        const uint32_t k = at + __popc(m & ((1u << c) - 1u));
+        buf[k] = DevPair{slot0 + c, qid};
+        if constexpr (ROUTED) bat[k] = rb;
+      }
+    }
+    n += total;
+  }
+
+  // Packet scheme: every lane adds (slot, rid[j]) for each set bit j of hm;
+  // rbt[j] = batch of query j in a merged launch.
+  __device__ __forceinline__ void add_masks(const DevQueue& qu, uint32_t hm, uint32_t slot,
+                                            const uint32_t* rid, const uint32_t* rbt) {
+    if (!__any_sync(kFull, hm != 0)) return;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = __popc(hm);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(kFull, incl, o);
+      if (lane >= static_cast<uint32_t>(o)) incl += v;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (n + total > kWarpOutCap) flush(qu);
+    if (total > kWarpOutCap) {  // more than a buffer: straight to the queues
+      if (hm == 0) return;
+      const uint32_t gid = __ldg(ids + slot);
+      if constexpr (ROUTED) {
+        while (hm) {
+          const uint32_t j = __ffs(hm) - 1;
+          hm &= hm - 1;
+          const DevQueue Q = routes[rbt[j]];
+          const unsigned long long p = atomicAdd(Q.size, 1u);
+          if (p < Q.capacity) Q.data[p] = DevPair{gid, __ldg(ident + rid[j])};
+        }
+      } else {
+        unsigned long long p = atomicAdd(qu.size, cnt);
+        while (hm) {
+          const uint32_t j = __ffs(hm) - 1;
+          hm &= hm - 1;
+          if (p < qu.capacity) qu.data[p] = DevPair{gid, rid[j]};
+          ++p;
+        }
+      }
+      return;
+    }
+    uint32_t k = n + incl - cnt;
+    while (hm) {
+      const uint32_t j = __ffs(hm) - 1;
+      hm &= hm - 1;
+      buf[k] = DevPair{slot, rid[j]};
+      if constexpr (ROUTED) bat[k] = rbt[j];
+      ++k;
+    }
     n += total;
   }
 
   // Team scheme: each lane has at most one pair (its leaf slot).
   __device__ __forceinline__ void add_one(const DevQueue& qu, bool hit, uint32_t slot,
-                                          uint32_t qid) {
+                                          uint32_t qid, uint32_t rb) {
     const uint32_t bal = __ballot_sync(kFull, hit);
     if (bal == 0) return;
     const uint32_t total = __popc(bal);
     if (n + total > kWarpOutCap) flush(qu);
-    if (hit) buf[n + __popc(bal & ((1u << lane_id()) - 1u))] = DevPair{slot, qid};
+    if (hit) {
+      const uint32_t k = n + __popc(bal & lanemask_lt());
+      buf[k] = DevPair{slot, qid};
+      if constexpr (ROUTED) bat[k] = rb;
+    }
     n += total;
   }
 };

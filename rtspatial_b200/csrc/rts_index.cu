@@ -252,13 +252,15 @@ LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   (void)pred;
   p.frontier = (trav == RTS_TRAVERSAL_FRONTIER);
   p.team = (trav == RTS_TRAVERSAL_TEAM);
+  p.packet = (trav == RTS_TRAVERSAL_PACKET);
   // Work items: the configured chunk, shrunk for small launches so that every
   // resident warp (about 32 per SM) still gets a few chunks.
   uint32_t chunk = ix->cfg.chunk ? ix->cfg.chunk : 128u;
   const uint64_t warps = static_cast<uint64_t>(device_sm_count()) * 32;
   const uint64_t fair = ((total + 4 * warps - 1) / (4 * warps) + 31) / 32 * 32;
   p.chunk = static_cast<uint32_t>(std::max<uint64_t>(32, std::min<uint64_t>(chunk, fair)));
-  p.high_occupancy = ix->cfg.query_occupancy >= 4;
+  const int occ = ix->cfg.query_occupancy;
+  p.min_blocks = occ >= 4 ? 4 : (occ >= 2 ? 2 : 1);
   return p;
 }
 
@@ -268,18 +270,33 @@ bool want_sort(const rts_index* ix, uint64_t total) {
   return total >= 8192;  // auto: small launches are latency-bound, skip the sort
 }
 
-// Assigns each batch its slice of the launch's visiting order (qbase, order)
-// and reserves the sort scratch.  Call before the descriptors are staged.
-int plan_order(QueryScratch& qs, BatchDesc* descs, uint32_t nd, uint64_t total, cudaStream_t s) {
+bool merge_batches(const LaunchPlan& plan, const BatchDesc* descs, uint32_t nd) {
+  if (nd < 2 || plan.frontier || plan.team) return false;
+  for (uint32_t i = 1; i < nd; ++i)
+    if (descs[i].pred != descs[0].pred || descs[i].mode != descs[0].mode) return false;
+  // Measured on B200: routing pays for counting and for the packet scheme
+  // (which needs spatially coherent packets); the thread scheme collects
+  // faster batch by batch.
+  return descs[0].mode == kCount || plan.packet;
+}
+
+int plan_order(QueryScratch& qs, const LaunchPlan& plan, BatchDesc* descs, uint32_t nd,
+               uint64_t total, cudaStream_t s) {
   int rc;
   if ((rc = buf_reserve(qs.keys_a, total * 8, s, false, 0))) return rc;
   if ((rc = buf_reserve(qs.keys_b, total * 8, s, false, 0))) return rc;
   if ((rc = buf_reserve(qs.vals, total * 4, s, false, 0))) return rc;
   if ((rc = buf_reserve(qs.order, total * 4, s, false, 0))) return rc;
+  if (plan.merged) {
+    if ((rc = buf_reserve(qs.m_queries, total * 16, s, false, 0))) return rc;
+    if ((rc = buf_reserve(qs.m_batch, total * 4, s, false, 0))) return rc;
+    if ((rc = buf_reserve(qs.m_ident, total * 4, s, false, 0))) return rc;
+    if ((rc = buf_reserve(qs.m_routes, nd * sizeof(DevQueue), s, false, 0))) return rc;
+  }
   uint64_t q = 0;
   for (uint32_t i = 0; i < nd; ++i) {
     descs[i].qbase = static_cast<uint32_t>(q);
-    descs[i].order = static_cast<const uint32_t*>(qs.order.ptr) + q;
+    descs[i].order = plan.merged ? nullptr : static_cast<const uint32_t*>(qs.order.ptr) + q;
     q += descs[i].n;
   }
   return RTS_OK;
@@ -287,14 +304,18 @@ int plan_order(QueryScratch& qs, BatchDesc* descs, uint32_t nd, uint64_t total, 
 
 // Fills the visiting order planned by plan_order (descriptors already on the
 // device when nd > 1).
-int fill_order(rts_index* ix, QueryScratch& qs, const BatchDesc* host, const BatchDesc* dev,
-               uint32_t nd, uint64_t total, cudaStream_t s) {
+int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const BatchDesc* host,
+               const BatchDesc* dev, uint32_t nd, uint64_t total, cudaStream_t s) {
   return launch_query_order(dev, host[0], nd, total,
                             static_cast<const float4*>(ix->trees[0].nodes.ptr), ix->cfg.curve,
                             static_cast<unsigned long long*>(qs.keys_a.ptr),
                             static_cast<unsigned long long*>(qs.keys_b.ptr),
                             static_cast<uint32_t*>(qs.vals.ptr),
-                            static_cast<uint32_t*>(qs.order.ptr), qs.sort_temp, s);
+                            static_cast<uint32_t*>(qs.order.ptr), qs.sort_temp, s, plan.merged,
+                            qs.m_queries.ptr, static_cast<uint32_t*>(qs.m_batch.ptr),
+                            static_cast<uint32_t*>(qs.m_ident.ptr),
+                            host[0].mode == kCollect ? static_cast<DevQueue*>(qs.m_routes.ptr)
+                                                     : nullptr);
 }
 
 // Turns public batch descriptions into launch descriptors (validating them);
@@ -379,6 +400,20 @@ int run_launch(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
   for (uint32_t i = 1; i < nd && uniform; ++i)
     uniform = descs[i].pred == descs[0].pred && descs[i].mode == descs[0].mode;
   auto* work = static_cast<uint32_t*>(qs.work.ptr);
+  if (plan.merged) {
+    // One batch: the sorted copy of every query; results routed per query.
+    BatchDesc v{};
+    v.queries = static_cast<const float*>(qs.m_queries.ptr);
+    v.n = static_cast<uint32_t>(total);
+    v.pred = descs[0].pred;
+    v.mode = descs[0].mode;
+    const MergedOrder mo{dd, static_cast<const uint32_t*>(qs.m_batch.ptr),
+                         static_cast<const uint32_t*>(qs.m_ident.ptr),
+                         static_cast<const DevQueue*>(qs.m_routes.ptr)};
+    const uint64_t mchunks = (total + plan.chunk - 1) / plan.chunk;
+    return launch_queries(ix->forest, plan, &v, nullptr, 1, static_cast<uint32_t>(mchunks), work,
+                          s, nullptr, nullptr, &mo);
+  }
   if (!uniform)
     return launch_queries(ix->forest, plan, descs, dd, nd, static_cast<uint32_t>(chunks), work, s);
   int rc = reserve_frontier(ix, qs, total, s);
@@ -423,11 +458,11 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   b.chunk_begin = 0;
   b.order = nullptr;
   b.qbase = 0;
-  if (want_sort(ix, n)) {
-    if ((rc = plan_order(ix->qs, &b, 1, n, s))) return rc;
-    if ((rc = fill_order(ix, ix->qs, &b, nullptr, 1, n, s))) return rc;
-  }
   LaunchPlan plan = plan_for(ix, pred, n);
+  if (want_sort(ix, n)) {
+    if ((rc = plan_order(ix->qs, plan, &b, 1, n, s))) return rc;
+    if ((rc = fill_order(ix, ix->qs, plan, &b, nullptr, 1, n, s))) return rc;
+  }
   uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
   return run_launch(ix, ix->qs, plan, &b, nullptr, 1, n, chunks, s);
 }
@@ -472,7 +507,7 @@ int rts_create(const rts_config* cfg, rts_index** out) {
   if (cfg) c = *cfg; else rts_config_default(&c);
   if (c.node_width != 4 && c.node_width != 8 && c.node_width != 16 && c.node_width != 32)
     return fail(RTS_ERR_INVALID_ARGUMENT, "node_width must be 4, 8, 16 or 32");
-  if (c.traversal < 0 || c.traversal > RTS_TRAVERSAL_FRONTIER)
+  if (c.traversal < 0 || c.traversal > RTS_TRAVERSAL_PACKET)
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad traversal");
   if (c.curve != RTS_CURVE_MORTON && c.curve != RTS_CURVE_HILBERT)
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad curve");
@@ -626,13 +661,15 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   uint64_t total = 0;
   for (const auto& d : descs) total += d.n;
   const bool sorted = want_sort(ix, total);
-  if (sorted && (rc = plan_order(ix->qs, descs.data(), static_cast<uint32_t>(descs.size()), total, s)))
+  plan.merged = sorted && merge_batches(plan, descs.data(), static_cast<uint32_t>(descs.size()));
+  if (sorted && (rc = plan_order(ix->qs, plan, descs.data(), static_cast<uint32_t>(descs.size()),
+                                 total, s)))
     return rc;
   void* ddev = nullptr;
   if (descs.size() > 1 &&
       (rc = ix->staging.put(descs.data(), descs.size() * sizeof(BatchDesc), s, &ddev)))
     return rc;
-  if (sorted && (rc = fill_order(ix, ix->qs, descs.data(), static_cast<const BatchDesc*>(ddev),
+  if (sorted && (rc = fill_order(ix, ix->qs, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
                                  static_cast<uint32_t>(descs.size()), total, s)))
     return rc;
   return run_launch(ix, ix->qs, plan, descs.data(), static_cast<const BatchDesc*>(ddev),

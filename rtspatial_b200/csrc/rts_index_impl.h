@@ -64,12 +64,15 @@ struct Staging {
 // own QueryScratch.
 struct QueryScratch {
   DevBuf work, keys_a, keys_b, vals, order, sort_temp;
+  // merged launch: queries in sorted order, their batch and reported id
+  DevBuf m_queries, m_batch, m_ident, m_routes;
   // frontier traversal
   DevBuf fr_qbuf, fr_qaux, fr_qbatch, fr_vis, fr_a, fr_b, fr_counts, fr_spill, fr_any;
   FrontierBufs fb;
   void release(cudaStream_t s) {
-    DevBuf* all[] = {&work, &keys_a, &keys_b, &vals, &order, &sort_temp, &fr_qbuf, &fr_qaux,
-                     &fr_qbatch, &fr_vis, &fr_a, &fr_b, &fr_counts, &fr_spill, &fr_any};
+    DevBuf* all[] = {&work, &keys_a, &keys_b, &vals, &order, &sort_temp, &m_queries, &m_batch,
+                     &m_ident, &m_routes, &fr_qbuf, &fr_qaux, &fr_qbatch, &fr_vis, &fr_a, &fr_b,
+                     &fr_counts, &fr_spill, &fr_any};
     for (DevBuf* b : all) buf_free(*b, s);
   }
 };
@@ -116,9 +119,17 @@ uint64_t sum_queries(const rts_batch* batches, uint32_t n);
 void keep_pool_memory();
 bool want_sort(const rts_index* ix, uint64_t total);
 int check_handler(int handler, void* arg);
-int plan_order(QueryScratch& qs, BatchDesc* descs, uint32_t nd, uint64_t total, cudaStream_t s);
-int fill_order(rts_index* ix, QueryScratch& qs, const BatchDesc* host, const BatchDesc* dev,
-               uint32_t nd, uint64_t total, cudaStream_t s);
+// Whether a sorted launch of these batches runs merged: more than one batch,
+// all of one predicate and handler, the thread or packet scheme, and either
+// the counting handler or the packet scheme.
+bool merge_batches(const LaunchPlan& plan, const BatchDesc* descs, uint32_t nd);
+// Reserves the sort (and, when plan.merged, the merged-query) scratch and
+// assigns each batch its slice of the launch's visiting order.  Call before
+// the descriptors are staged.
+int plan_order(QueryScratch& qs, const LaunchPlan& plan, BatchDesc* descs, uint32_t nd,
+               uint64_t total, cudaStream_t s);
+int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const BatchDesc* host,
+               const BatchDesc* dev, uint32_t nd, uint64_t total, cudaStream_t s);
 int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
                const LaunchPlan& plan, std::vector<BatchDesc>& out, uint64_t& chunks);
 // Sizes the frontier buffers of `qs` for `total` queries (no-op when large

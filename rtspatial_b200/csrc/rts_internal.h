@@ -73,11 +73,18 @@ int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint
                      cudaStream_t s);
 // Visiting order of the queries of nb batches: sorts (batch, curve key of the
 // query centre) and writes each batch's query indices to order[qbase ...].
+// With `merged` (every batch of one predicate, nb > 1) the queries of all
+// batches are sorted together and copied in sorted order to merged_q (float4,
+// or float2 for points), with each position's batch index and reported id;
+// for collecting batches merged_routes[b] receives a copy of batch b's queue.
 int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
                        const float4* frame_box, int curve, unsigned long long* keys_a,
                        unsigned long long* keys_b, uint32_t* vals_a, uint32_t* order,
-                       DevBuf& temp, cudaStream_t s);
-// Temporary bytes the order sort of `total` queries in `nb` batches needs.
+                       DevBuf& temp, cudaStream_t s, bool merged = false, void* merged_q = nullptr,
+                       uint32_t* merged_batch = nullptr, uint32_t* merged_ident = nullptr,
+                       DevQueue* merged_routes = nullptr);
+// Temporary bytes the order sort of `total` queries in `nb` batches needs
+// (an upper bound for the merged sort too).
 int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes);
 int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
                   float4* leaves, cudaStream_t s);
@@ -111,8 +118,10 @@ struct LaunchPlan {
   int width = 8;
   bool team = false;
   bool frontier = false;      // breadth-first pass (plus depth-first fallback)
+  bool packet = false;        // warp-per-packet depth-first scheme
   uint32_t chunk = 32;  // queries per work item
-  bool high_occupancy = false;  // cap registers for 4 CTAs of 256 threads per SM
+  int min_blocks = 1;         // CTAs of 256 threads per SM the registers are capped for (1, 2, 4)
+  bool merged = false;        // sort the queries of all batches together (MergedOrder)
 };
 // Runs `nb` batches (descriptors in host memory `hb`; device copy `db` when
 // nb > 1) in one persistent launch.  work_counter: zeroed device uint32.
@@ -121,10 +130,13 @@ struct LaunchPlan {
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
                    uint32_t* work_counter, cudaStream_t s, const uint32_t* only = nullptr,
-                   const uint32_t* only_any = nullptr);
+                   const uint32_t* only_any = nullptr, const MergedOrder* merged = nullptr);
+// Sets the chosen query kernel's shared-memory limit on the current device
+// (once; call outside stream capture before a launch is captured).
+int prepare_query_kernel(const LaunchPlan& plan);
 // Number of SMs of the current device (cached).
 int device_sm_count();
 // Resident CTAs per SM of the chosen query kernel (for sizing the grid).
-int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks);
+int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks, bool merged = false);
 
 }  // namespace rts

@@ -41,7 +41,7 @@ int enqueue(rts_plan* p, cudaStream_t s) {
   const uint32_t nd = static_cast<uint32_t>(p->descs.size());
   const BatchDesc* dd = static_cast<const BatchDesc*>(p->ddescs.ptr);
   int rc;
-  if (p->sorted && (rc = fill_order(ix, p->qs, p->descs.data(), nd > 1 ? dd : nullptr, nd,
+  if (p->sorted && (rc = fill_order(ix, p->qs, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd,
                                     p->total, s)))
     return rc;
   return run_launch(ix, p->qs, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd, p->total,
@@ -70,12 +70,16 @@ int rts_plan_create(rts_index* ix, const rts_batch* batches, uint32_t n_batches,
   if (!rc) rc = buf_reserve(p->qs.work, sizeof(uint32_t), s, false, 0);
   p->sorted = !p->descs.empty() && want_sort(ix, p->total);
   if (!rc && p->sorted) {
-    rc = plan_order(p->qs, p->descs.data(), static_cast<uint32_t>(p->descs.size()), p->total, s);
+    p->plan.merged =
+        merge_batches(p->plan, p->descs.data(), static_cast<uint32_t>(p->descs.size()));
+    rc = plan_order(p->qs, p->plan, p->descs.data(), static_cast<uint32_t>(p->descs.size()),
+                    p->total, s);
     size_t need = 0;
     if (!rc) rc = query_order_temp_bytes(p->total, static_cast<uint32_t>(p->descs.size()), &need);
     if (!rc) rc = buf_reserve(p->qs.sort_temp, need, s, false, 0);
   }
   if (!rc && p->plan.frontier && !p->descs.empty()) rc = reserve_frontier(ix, p->qs, p->total, s);
+  if (!rc) rc = prepare_query_kernel(p->plan);
   if (!rc && !p->descs.empty()) {
     size_t bytes = p->descs.size() * sizeof(BatchDesc);
     rc = buf_reserve(p->ddescs, bytes, s, false, 0);

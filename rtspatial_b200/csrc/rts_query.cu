@@ -7,51 +7,55 @@
 // width W).  Predicate and handler are per batch, so one launch can mix
 // point-contains, range-contains and range-intersects batches, each writing
 // to its own counter or queue with its own 0-based query ids.
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "rts_internal.h"
 
 namespace rts {
 
-template <int W, bool TEAM, int PRED, int MODE>
+template <int W, bool TEAM, bool ROUTED, int PRED, int MODE>
 __device__ __forceinline__ void run_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                          uint32_t ce, DevPair* wbuf, const uint32_t* only) {
+                                          uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                          const uint32_t* only, const MergedOrder& M) {
   if constexpr (TEAM) {
-    run_chunk_team<PRED, MODE, W>(F, B, cb, ce, wbuf, only);
+    run_chunk_team<PRED, MODE, W>(F, B, cb, ce, wbuf, wbat, only);
   } else {
-    run_chunk_thread<PRED, MODE, W>(F, B, cb, ce, wbuf, only);
+    run_chunk_thread<PRED, MODE, W, ROUTED>(F, B, cb, ce, wbuf, wbat, only, M);
   }
 }
 
-template <int W, bool TEAM>
+template <int W, bool TEAM, bool ROUTED>
 __device__ __noinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                            uint32_t ce, DevPair* wbuf, const uint32_t* only) {
+                                            uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                            const uint32_t* only, const MergedOrder& M) {
+#define RTS_RUN(P, H) run_chunk<W, TEAM, ROUTED, P, H>(F, B, cb, ce, wbuf, wbat, only, M)
   switch (B.pred * 2 + B.mode) {
-    case kPoint * 2 + kCount: run_chunk<W, TEAM, kPoint, kCount>(F, B, cb, ce, wbuf, only); break;
-    case kPoint * 2 + kCollect: run_chunk<W, TEAM, kPoint, kCollect>(F, B, cb, ce, wbuf, only); break;
-    case kContains * 2 + kCount: run_chunk<W, TEAM, kContains, kCount>(F, B, cb, ce, wbuf, only); break;
-    case kContains * 2 + kCollect:
-      run_chunk<W, TEAM, kContains, kCollect>(F, B, cb, ce, wbuf, only);
-      break;
-    case kIntersects * 2 + kCount:
-      run_chunk<W, TEAM, kIntersects, kCount>(F, B, cb, ce, wbuf, only);
-      break;
-    case kIntersects * 2 + kCollect:
-      run_chunk<W, TEAM, kIntersects, kCollect>(F, B, cb, ce, wbuf, only);
-      break;
+    case kPoint * 2 + kCount: RTS_RUN(kPoint, kCount); break;
+    case kPoint * 2 + kCollect: RTS_RUN(kPoint, kCollect); break;
+    case kContains * 2 + kCount: RTS_RUN(kContains, kCount); break;
+    case kContains * 2 + kCollect: RTS_RUN(kContains, kCollect); break;
+    case kIntersects * 2 + kCount: RTS_RUN(kIntersects, kCount); break;
+    case kIntersects * 2 + kCollect: RTS_RUN(kIntersects, kCollect); break;
     default: break;
   }
+#undef RTS_RUN
 }
 
 constexpr int kQueryThreads = 256;
 
-template <int W, bool TEAM, int MINB>
+// ROUTED: a merged launch (results routed per query); thread scheme only.
+template <int W, bool TEAM, int MINB, bool ROUTED>
 __global__ void __launch_bounds__(kQueryThreads, MINB)
     k_query(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
             const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
             uint32_t chunk, uint32_t* __restrict__ work, const uint32_t* __restrict__ only,
-            const uint32_t* __restrict__ only_any) {
+            const uint32_t* __restrict__ only_any, const __grid_constant__ MergedOrder M) {
   if (only_any && *only_any == 0) return;
   __shared__ Forest F;
   __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
+  extern __shared__ __align__(16) unsigned char qdyn[];  // merged launch: batch tables
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&F_in);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&F);
@@ -77,35 +81,121 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     }
     const uint32_t cb = (c - B.chunk_begin) * chunk;
     const uint32_t ce = min(cb + chunk, B.n);
-    dispatch_chunk<W, TEAM>(F, B, cb, ce, wbufs[threadIdx.x / 32], only);
+    uint32_t* wbat =
+        ROUTED ? reinterpret_cast<uint32_t*>(qdyn) + (threadIdx.x / 32) * kWarpBatWords : nullptr;
+    dispatch_chunk<W, TEAM, ROUTED>(F, B, cb, ce, wbufs[threadIdx.x / 32], wbat, only, M);
+  }
+}
+
+template <int W, bool ROUTED>
+__device__ __noinline__ void dispatch_packet(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                             uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                             void* praw, const MergedOrder& M) {
+#define RTS_RUN(P, H) run_chunk_packet<P, H, W, ROUTED>(F, B, cb, ce, wbuf, wbat, praw, M)
+  switch (B.pred * 2 + B.mode) {
+    case kPoint * 2 + kCount: RTS_RUN(kPoint, kCount); break;
+    case kPoint * 2 + kCollect: RTS_RUN(kPoint, kCollect); break;
+    case kContains * 2 + kCount: RTS_RUN(kContains, kCount); break;
+    case kContains * 2 + kCollect: RTS_RUN(kContains, kCollect); break;
+    case kIntersects * 2 + kCount: RTS_RUN(kIntersects, kCount); break;
+    case kIntersects * 2 + kCollect: RTS_RUN(kIntersects, kCollect); break;
+    default: break;
+  }
+#undef RTS_RUN
+}
+
+template <int W>
+constexpr size_t packet_stride() {
+  return (packet_smem_bytes<W>() + 15) / 16 * 16;
+}
+
+// Packet scheme: same work distribution as k_query; each warp walks its
+// chunk 32 queries at a time.  (No query filter: the frontier's fallback uses
+// the other schemes.)
+template <int W, int MINB, bool ROUTED>
+__global__ void __launch_bounds__(kQueryThreads, MINB)
+    k_query_packet(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
+                   const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
+                   uint32_t chunk, uint32_t* __restrict__ work, const uint32_t* __restrict__,
+                   const uint32_t* __restrict__, const __grid_constant__ MergedOrder M) {
+  __shared__ Forest F;
+  __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
+  // packet_stride<W>() per warp, then (merged launch) the warps' batch tables
+  extern __shared__ __align__(16) unsigned char qdyn[];
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&F_in);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&F);
+    for (uint32_t i = threadIdx.x; i < sizeof(Forest) / 4; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const uint32_t lane = lane_id();
+  const uint32_t wid = threadIdx.x / 32;
+  for (;;) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(work, 1u);
+    c = __shfl_sync(kFull, c, 0);
+    if (c >= total_chunks) break;
+    BatchDesc B;
+    if (nb == 1) {
+      B = b0;
+    } else {
+      uint32_t lo = 0, hi = nb - 1;  // largest b with chunk_begin <= c
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&descs[mid].chunk_begin) <= c) lo = mid; else hi = mid - 1;
+      }
+      B = descs[lo];
+    }
+    const uint32_t cb = (c - B.chunk_begin) * chunk;
+    const uint32_t ce = min(cb + chunk, B.n);
+    unsigned char* praw = qdyn + wid * packet_stride<W>();
+    uint32_t* wbat = ROUTED ? reinterpret_cast<uint32_t*>(
+                                  qdyn + (kQueryThreads / 32) * packet_stride<W>()) +
+                                  wid * kWarpBatWords
+                            : nullptr;
+    dispatch_packet<W, ROUTED>(F, B, cb, ce, wbufs[wid], wbat, praw, M);
   }
 }
 
 using QueryKernel = void (*)(const Forest, const BatchDesc, const BatchDesc*, uint32_t, uint32_t,
-                             uint32_t, uint32_t*, const uint32_t*, const uint32_t*);
+                             uint32_t, uint32_t*, const uint32_t*, const uint32_t*,
+                             const MergedOrder);
 
-template <int MINB>
+template <int MINB, bool ROUTED>
 static QueryKernel pick_kernel_occ(const LaunchPlan& p) {
-  if (p.team) {
+  if (p.packet) {
     switch (p.width) {
-      case 4: return k_query<4, true, MINB>;
-      case 8: return k_query<8, true, MINB>;
-      case 16: return k_query<16, true, MINB>;
-      case 32: return k_query<32, true, MINB>;
+      case 4: return k_query_packet<4, MINB, ROUTED>;
+      case 8: return k_query_packet<8, MINB, ROUTED>;
+      case 16: return k_query_packet<16, MINB, ROUTED>;
+      case 32: return k_query_packet<32, MINB, ROUTED>;
+    }
+  } else if (p.team) {
+    if constexpr (!ROUTED) {
+      switch (p.width) {
+        case 4: return k_query<4, true, MINB, false>;
+        case 8: return k_query<8, true, MINB, false>;
+        case 16: return k_query<16, true, MINB, false>;
+        case 32: return k_query<32, true, MINB, false>;
+      }
     }
   } else {
     switch (p.width) {
-      case 4: return k_query<4, false, MINB>;
-      case 8: return k_query<8, false, MINB>;
-      case 16: return k_query<16, false, MINB>;
-      case 32: return k_query<32, false, MINB>;
+      case 4: return k_query<4, false, MINB, ROUTED>;
+      case 8: return k_query<8, false, MINB, ROUTED>;
+      case 16: return k_query<16, false, MINB, ROUTED>;
+      case 32: return k_query<32, false, MINB, ROUTED>;
     }
   }
   return nullptr;
 }
 
-static QueryKernel pick_kernel(const LaunchPlan& p) {
-  return p.high_occupancy ? pick_kernel_occ<4>(p) : pick_kernel_occ<1>(p);
+static QueryKernel pick_kernel(const LaunchPlan& p, bool routed) {
+  switch (p.min_blocks) {
+    case 4: return routed ? pick_kernel_occ<4, true>(p) : pick_kernel_occ<4, false>(p);
+    case 2: return routed ? pick_kernel_occ<2, true>(p) : pick_kernel_occ<2, false>(p);
+    default: return routed ? pick_kernel_occ<1, true>(p) : pick_kernel_occ<1, false>(p);
+  }
 }
 
 static int g_num_sms = 0;
@@ -120,12 +210,51 @@ int device_sm_count() {
   return g_num_sms;
 }
 
-int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks) {
-  QueryKernel k = pick_kernel(plan);
+// Dynamic shared memory of the chosen kernel: the packet scheme's per-warp
+// query tables, and the per-warp batch tables of a merged launch.
+static size_t dyn_smem_bytes(const LaunchPlan& p, bool merged) {
+  size_t per = 0;
+  if (p.packet) {
+    switch (p.width) {
+      case 4: per = packet_stride<4>(); break;
+      case 8: per = packet_stride<8>(); break;
+      case 16: per = packet_stride<16>(); break;
+      case 32: per = packet_stride<32>(); break;
+    }
+  }
+  if (merged) per += kWarpBatWords * sizeof(uint32_t);
+  return per * (kQueryThreads / 32);
+}
+
+// Raises the kernel's dynamic shared-memory limit (to its largest use) once
+// per device.
+static int prepare_kernel(QueryKernel k, size_t dyn) {
+  if (dyn == 0) return RTS_OK;
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  RTS_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(dev, reinterpret_cast<const void*>(k));
+  if (done.count(key)) return RTS_OK;
+  RTS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(dyn)));
+  done.insert(key);
+  return RTS_OK;
+}
+
+int prepare_query_kernel(const LaunchPlan& plan) {
+  QueryKernel k = pick_kernel(plan, plan.merged);
+  return k ? prepare_kernel(k, dyn_smem_bytes(plan, plan.merged)) : RTS_OK;
+}
+
+int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks, bool merged) {
+  QueryKernel k = pick_kernel(plan, merged);
   if (!k) return 0;
   device_sm_count();
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kQueryThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kQueryThreads,
+                                                dyn_smem_bytes(plan, merged));
   if (per_sm <= 0) per_sm = 1;
   const uint32_t warps_per_block = kQueryThreads / 32;
   uint64_t want = (static_cast<uint64_t>(total_chunks) + warps_per_block - 1) / warps_per_block;
@@ -136,14 +265,20 @@ int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks) {
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
                    uint32_t* work_counter, cudaStream_t s, const uint32_t* only,
-                   const uint32_t* only_any) {
+                   const uint32_t* only_any, const MergedOrder* merged) {
   if (total_chunks == 0) return RTS_OK;
-  QueryKernel k = pick_kernel(plan);
+  LaunchPlan use = plan;
+  if (only) use.packet = false;  // the packet scheme takes no query filter
+  QueryKernel k = pick_kernel(use, merged != nullptr);
   if (!k) return fail(RTS_ERR_INVALID_ARGUMENT, "unsupported node width / traversal");
-  int grid = query_grid_size(plan, total_chunks);
+  const size_t dyn = dyn_smem_bytes(use, merged != nullptr);
+  int rc = prepare_kernel(k, dyn);
+  if (rc) return rc;
+  int grid = query_grid_size(use, total_chunks, merged != nullptr);
   RTS_CUDA_TRY(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), s));
-  k<<<grid, kQueryThreads, 0, s>>>(F, hb[0], db, nb, total_chunks, plan.chunk, work_counter, only,
-                                   only_any);
+  const MergedOrder M = merged ? *merged : MergedOrder{nullptr, nullptr, nullptr, nullptr};
+  k<<<grid, kQueryThreads, dyn, s>>>(F, hb[0], db, nb, total_chunks, plan.chunk, work_counter,
+                                     only, only_any, M);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }

@@ -356,7 +356,7 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
   }
   int rc = RTS_OK;
   const bool sorted = want_sort(ix, total);
-  if (sorted) rc = plan_order(sl.qs, sl.h_descs, np, total, s);
+  if (sorted) rc = plan_order(sl.qs, plan, sl.h_descs, np, total, s);
   cudaError_t e = cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, in_used, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(sl.d_queues.ptr, sl.h_queues, np * sizeof(DevQueue), cudaMemcpyHostToDevice, s);
@@ -366,7 +366,7 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
   if (e != cudaSuccess) rc = cuda_fail(e, "server launch staging");
   refresh_forest(ix);
   const BatchDesc* dd = static_cast<const BatchDesc*>(sl.d_descs.ptr);
-  if (!rc && sorted) rc = fill_order(ix, sl.qs, sl.h_descs, np > 1 ? dd : nullptr, np, total, s);
+  if (!rc && sorted) rc = fill_order(ix, sl.qs, plan, sl.h_descs, np > 1 ? dd : nullptr, np, total, s);
   if (!rc)
     rc = launch_queries(ix->forest, plan, sl.h_descs, np > 1 ? dd : nullptr, np,
                         static_cast<uint32_t>(chunks), static_cast<uint32_t*>(sl.qs.work.ptr), s);

@@ -13,36 +13,20 @@
 // (or teams) whose query is finished take the next unstarted query of the
 // chunk at the end of each step (ballot + popc ranking), so the warp stays
 // full while the chunk lasts even when per-query work is heavily skewed.
+// In a merged launch (MergedOrder) the batch is the launch's sorted query
+// array and results are routed to each query's own batch.
 #pragma once
 
 #include "rts_device.cuh"
 
 namespace rts {
 
-// Parameters of one batch (one reference Query call).
-struct BatchDesc {
-  const float* queries;
-  void* arg;              // counter (count) or DevQueue* (collect)
-  uint32_t n;             // queries in the batch
-  int32_t pred;           // PredKind
-  int32_t mode;           // HandlerKind
-  uint32_t chunk_begin;   // index of the batch's first chunk in the launch
-  const uint32_t* order;  // optional visiting order (query ids), or nullptr
-  uint32_t qbase;         // offset of the batch in the launch's concatenated order
-  uint32_t id_offset;     // added to every reported query id (0 for a Query call)
-};
-
-__device__ __forceinline__ uint32_t lanemask_lt() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
 template <int PRED, int W>
 struct TravState {
   typename QueryOps<PRED>::Q q;
   MaskStack<W> ms;
-  uint32_t qid;   // id reported for this query
+  uint32_t qid;   // id reported for this query (merged launch: sorted position)
+  uint32_t rb;    // merged launch: the query's batch
   uint32_t t;     // tree
   uint32_t L;     // level of the group being visited
   uint32_t g;     // group index at level L
@@ -50,10 +34,12 @@ struct TravState {
 
 // Starts query qid (visiting slot `slot` of the batch) at the top of tree 0.
 // Returns false when the forest is empty.
-template <int PRED, int W>
+template <int PRED, int W, bool ROUTED>
 __device__ __forceinline__ bool trav_start(const Forest& F, const BatchDesc& B, uint32_t slot,
-                                           TravState<PRED, W>& s, const uint32_t* only) {
+                                           TravState<PRED, W>& s, const uint32_t* only,
+                                           const MergedOrder& M) {
   s.qid = B.order ? B.order[slot] : slot;
+  s.rb = ROUTED ? __ldg(M.batch + slot) : 0u;
   if (only) {
     const uint32_t g = B.qbase + s.qid;
     if (!((__ldg(only + (g >> 5)) >> (g & 31)) & 1u)) return false;
@@ -103,10 +89,11 @@ __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>
 // ---------------------------------------------------------------------------
 // thread scheme
 // ---------------------------------------------------------------------------
-template <int PRED, int MODE, int W>
+template <int PRED, int MODE, int W, bool ROUTED>
 __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDesc& B,
-                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf,
-                                                 const uint32_t* only) {
+                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf, uint32_t* wbat,
+                                                 const uint32_t* only,
+                                                 const MergedOrder& M) {
   using Ops = QueryOps<PRED>;
   const uint32_t lane = lane_id();
   TravState<PRED, W> s;
@@ -114,12 +101,12 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
   bool active = false;
   {
     uint32_t slot = next + lane;
-    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+    if (slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
     next = min(cend, next + 32u);
   }
   DevQueue qu{};
-  if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
-  WarpOut out{wbuf, 0, F.ids_base};
+  if (MODE == kCollect && !ROUTED) qu = *static_cast<const DevQueue*>(B.arg);
+  WarpOut<ROUTED> out(wbuf, wbat, F.ids_base, M);
   unsigned long long cnt = 0;
 
   for (;;) {
@@ -128,7 +115,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       // refill again until the chunk is exhausted.
       if (next >= cend) break;
       uint32_t slot = next + lane;
-      if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+      if (slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
       next = min(cend, next + 32u);
       continue;
     }
@@ -161,21 +148,27 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       }
     }
     if (MODE == kCollect) {
-      out.template add<W>(qu, leafm, leafslot, s.qid + B.id_offset);
+      out.template add<W>(qu, leafm, leafslot, s.qid + B.id_offset, s.rb);
     } else {
       cnt += __popc(leafm);
     }
-    if (active) active = trav_advance<PRED, W>(F, s);
+    if (active) {
+      active = trav_advance<PRED, W>(F, s);
+      if (MODE == kCount && ROUTED && !active) {
+        count_routed(M, s.rb, cnt);
+        cnt = 0;
+      }
+    }
     // Refill finished lanes from the chunk.
     uint32_t idle = __ballot_sync(kFull, !active);
     if (idle != 0 && next < cend) {
       uint32_t slot = next + __popc(idle & lanemask_lt());
-      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+      if (!active && slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
       next = min(cend, next + __popc(idle));
     }
   }
   if (MODE == kCollect) out.flush(qu);
-  if (MODE == kCount) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
+  if (MODE == kCount && !ROUTED) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -183,7 +176,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
 // ---------------------------------------------------------------------------
 template <int PRED, int MODE, int W>
 __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc& B,
-                                               uint32_t cbeg, uint32_t cend, DevPair* wbuf,
+                                               uint32_t cbeg, uint32_t cend, DevPair* wbuf, uint32_t* wbat,
                                                const uint32_t* only) {
   using Ops = QueryOps<PRED>;
   constexpr uint32_t kTeams = 32 / W;
@@ -191,24 +184,25 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
   const uint32_t lane = lane_id();
   const uint32_t team = lane / W;
   const uint32_t tl = lane % W;
+  const MergedOrder M{};  // the team scheme runs batch by batch
   TravState<PRED, W> s;
   uint32_t next = cbeg;
   bool active = false;
   {
     uint32_t slot = next + team;
-    if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+    if (slot < cend) active = trav_start<PRED, W, false>(F, B, slot, s, only, M);
     next = min(cend, next + kTeams);
   }
   DevQueue qu{};
   if (MODE == kCollect) qu = *static_cast<const DevQueue*>(B.arg);
-  WarpOut out{wbuf, 0, F.ids_base};
+  WarpOut<false> out(wbuf, wbat, F.ids_base, M);
   unsigned long long cnt = 0;
 
   for (;;) {
     if (!__any_sync(kFull, active)) {
       if (next >= cend) break;  // see run_chunk_thread
       uint32_t slot = next + team;
-      if (slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+      if (slot < cend) active = trav_start<PRED, W, false>(F, B, slot, s, only, M);
       next = min(cend, next + kTeams);
       continue;
     }
@@ -229,7 +223,7 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
     }
     const uint32_t bal = __ballot_sync(kFull, hit);
     if (MODE == kCollect) {
-      out.add_one(qu, leaf_hit, gid, s.qid + B.id_offset);
+      out.add_one(qu, leaf_hit, gid, s.qid + B.id_offset, s.rb);
     } else {
       cnt += leaf_hit ? 1u : 0u;
     }
@@ -242,12 +236,194 @@ __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc&
     if (idle != 0 && next < cend) {
       uint32_t below = (team == 0) ? 0u : (idle & ((1u << (team * W)) - 1u));
       uint32_t slot = next + __popc(below) / W;
-      if (!active && slot < cend) active = trav_start<PRED, W>(F, B, slot, s, only);
+      if (!active && slot < cend) active = trav_start<PRED, W, false>(F, B, slot, s, only, M);
       next = min(cend, next + __popc(idle) / W);
     }
   }
   if (MODE == kCollect) out.flush(qu);
   if (MODE == kCount) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
+}
+
+}  // namespace rts
+
+namespace rts {
+
+// ---------------------------------------------------------------------------
+// packet scheme: one warp walks up to 32 queries together
+// ---------------------------------------------------------------------------
+// The warp descends the forest once for a packet of queries (consecutive in
+// the launch's visiting order, so spatially close when the order is sorted).
+// Lanes map to the W entries of the group being visited (32 / W queries are
+// tested per round when W < 32); each entry's test result is a 32-bit mask of
+// the packet's queries it satisfies.  An upper-level entry with a non-empty
+// mask becomes a group to visit with that mask; at the leaves the masks are
+// the packet's pairs.  Each group is loaded once per packet instead of once
+// per query, and every lane of a round does useful work.  The tests are the
+// ones the other schemes make (node test at upper levels, exact predicate at
+// the leaves), so results are identical.
+template <int PRED, int W>
+struct PacketSmem {
+  typename QueryOps<PRED>::Q q[32];  // the packet's queries (prepared per sub-tree)
+  uint32_t rid[32];                  // reported id (merged launch: sorted position)
+  uint32_t rb[32];                   // merged launch: batch of each query
+  uint32_t over[32];                 // merged counting: per-query carries out of the slices
+  uint32_t stk[MaskStack<W>::kLevels + 1][W];  // query masks of the path's pending entries
+};
+
+// Merged counting in the packet scheme: each entry lane keeps, for the 32
+// queries of the packet, how many of its entries' tests hit, as kSlices
+// bit-planes (bit j of plane k = bit k of query j's count), so adding a leaf
+// group's hit mask costs a few logic operations whatever the number of hits.
+constexpr int kSlices = 8;
+
+template <int W>
+constexpr size_t packet_smem_bytes() {
+  return sizeof(PacketSmem<kIntersects, W>) > sizeof(PacketSmem<kPoint, W>)
+             ? (sizeof(PacketSmem<kIntersects, W>) > sizeof(PacketSmem<kContains, W>)
+                    ? sizeof(PacketSmem<kIntersects, W>)
+                    : sizeof(PacketSmem<kContains, W>))
+             : sizeof(PacketSmem<kPoint, W>);
+}
+
+template <int PRED, int MODE, int W, bool ROUTED>
+__device__ __forceinline__ void run_chunk_packet(const Forest& F, const BatchDesc& B,
+                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf,
+                                                 uint32_t* wbat, void* praw,
+                                                 const MergedOrder& M) {
+  using Ops = QueryOps<PRED>;
+  using Q = typename Ops::Q;
+  constexpr uint32_t kGroups = 32 / W;  // queries tested per round
+  constexpr uint32_t kEntryMask = (W == 32) ? kFull : ((1u << W) - 1u);
+  PacketSmem<PRED, W>& P = *static_cast<PacketSmem<PRED, W>*>(praw);
+  const uint32_t lane = lane_id();
+  const uint32_t part = lane / W;  // which query of a round this lane tests
+  const uint32_t c = lane % W;     // which entry of the group
+  DevQueue qu{};
+  if (MODE == kCollect && !ROUTED) qu = *static_cast<const DevQueue*>(B.arg);
+  WarpOut<ROUTED> out(wbuf, wbat, F.ids_base, M);
+  unsigned long long cnt = 0;  // unmerged counting: this lane's pairs
+
+  for (uint32_t pk = cbeg; pk < cend; pk += 32) {
+    const uint32_t np = min(32u, cend - pk);
+    const uint32_t all = (np == 32) ? kFull : ((1u << np) - 1u);
+    Q myq{};
+    if (lane < np) {
+      const uint32_t slot = pk + lane;
+      const uint32_t qid = B.order ? B.order[slot] : slot;
+      myq = Ops::load(B.queries, qid);
+      P.rid[lane] = qid + B.id_offset;
+      P.rb[lane] = ROUTED ? __ldg(M.batch + slot) : 0u;
+    }
+    uint32_t planes[kSlices];  // merged counting: this lane's per-query counts, bit-sliced
+#pragma unroll
+    for (int k = 0; k < kSlices; ++k) planes[k] = 0;
+    P.over[lane] = 0;
+
+    for (uint32_t t = 0; t < F.n_trees; ++t) {
+      const TreeDesc& T = F.tree[t];
+      __syncwarp();
+      if (lane < np) {
+        Q qq = myq;
+        Ops::enter_tree(qq, __ldg(T.nodes));
+        P.q[lane] = qq;
+      }
+      __syncwarp();
+      MaskStack<W> pend;
+      pend.clear();
+      uint32_t L = T.top, g = 0, qm = all;
+      for (;;) {
+        // Visit group g of level L for the queries in qm.
+        const uint32_t first = g * W;
+        const bool at_leaf = (L == 0);
+        const float4* p = at_leaf ? T.leaves + first : T.nodes + T.level_off[L] + first;
+        const uint32_t lim = (at_leaf ? T.n : T.level_cnt[L]) - first;
+        const float4 e = __ldg(p + c);
+        const bool valid = c < lim;
+        uint32_t hm = 0;
+        uint32_t rm = qm;
+        while (rm) {  // uniform: kGroups queries per round
+          uint32_t mine = rm;
+#pragma unroll
+          for (uint32_t k = 0; k + 1 < kGroups; ++k)
+            if (k < part) mine &= mine - 1;
+#pragma unroll
+          for (uint32_t k = 0; k < kGroups; ++k) rm &= rm - 1;
+          if (mine && valid) {
+            const uint32_t j = __ffs(mine) - 1;
+            const bool hit = at_leaf ? Ops::leaf(e, P.q[j]) : Ops::node(e, P.q[j]);
+            if (hit) hm |= 1u << j;
+          }
+        }
+#pragma unroll
+        for (uint32_t o = W; o < 32; o <<= 1) hm |= __shfl_xor_sync(kFull, hm, o);
+        if (part != 0) hm = 0;  // lanes 0..W-1 own the entries from here on
+        if (at_leaf) {
+          const uint32_t slot0 = static_cast<uint32_t>(T.ids - F.ids_base) + first;
+          if (MODE == kCollect) {
+            out.add_masks(qu, hm, slot0 + c, P.rid, P.rb);
+          } else if (!ROUTED) {
+            cnt += __popc(hm);
+          } else {
+            uint32_t carry = hm;  // ripple-carry add of one hit per set bit
+#pragma unroll
+            for (int k = 0; k < kSlices; ++k) {
+              const uint32_t t = planes[k] & carry;
+              planes[k] ^= carry;
+              carry = t;
+            }
+            while (carry) {  // a count passed 2^kSlices - 1 (rare)
+              const uint32_t j = __ffs(carry) - 1;
+              carry &= carry - 1;
+              atomicAdd(&P.over[j], 1u);
+            }
+          }
+        } else {
+          if (part == 0) P.stk[L][c] = hm;
+          pend.set(L, __ballot_sync(kFull, hm != 0) & kEntryMask);
+        }
+        // Next group: the lowest pending entry of the deepest level that has one.
+        while (L == 0 || pend.get(L) == 0) {
+          if (L == T.top) break;
+          L += 1;
+          g /= W;
+        }
+        if (L == 0 || pend.get(L) == 0) break;  // sub-tree done
+        const uint32_t m = pend.get(L);
+        const uint32_t cc = __ffs(m) - 1;
+        pend.set(L, m & (m - 1));
+        __syncwarp();
+        qm = P.stk[L][cc];
+        g = g * W + cc;
+        L -= 1;
+      }
+    }
+    if (MODE == kCount && ROUTED) {
+      // Lane j gathers query j's count from every lane's planes.
+      unsigned long long qcount = 0;
+      uint32_t touched = 0;
+#pragma unroll
+      for (int k = 0; k < kSlices; ++k) touched |= planes[k];
+      touched = __reduce_or_sync(kFull, touched);
+      while (touched) {  // uniform
+        const uint32_t j = __ffs(touched) - 1;
+        touched &= touched - 1;
+        unsigned long long v = 0;
+#pragma unroll
+        for (int k = 0; k < kSlices; ++k)
+          v += static_cast<unsigned long long>(__popc(__ballot_sync(kFull, (planes[k] >> j) & 1u)))
+               << k;
+        if (lane == j) qcount = v;
+      }
+      __syncwarp();
+      if (lane < np) {
+        qcount += static_cast<unsigned long long>(P.over[lane]) << kSlices;
+        count_routed(M, P.rb[lane], qcount);
+      }
+    }
+    __syncwarp();
+  }
+  if (MODE == kCollect) out.flush(qu);
+  if (MODE == kCount && !ROUTED) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
 }
 
 }  // namespace rts

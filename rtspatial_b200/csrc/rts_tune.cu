@@ -1,6 +1,6 @@
 // Autotuner of the query launch: times candidate (node width, traversal
-// scheme, register cap, visiting order, chunk size) settings on a sample of
-// the caller's batches and keeps the fastest in the index.
+// scheme, register cap, visiting order, chunk size) settings on the caller's
+// batches and keeps the fastest in the index.
 //
 // The sample runs through the tuner's own counters and queues (a counting
 // pass sizes a pair buffer, then every candidate runs with the collecting
@@ -133,9 +133,13 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
       {RTS_TRAVERSAL_THREAD, 4, 0, 32},   {RTS_TRAVERSAL_THREAD, 4, 0, 64},
       {RTS_TRAVERSAL_THREAD, 4, 0, 128},  {RTS_TRAVERSAL_THREAD, 4, 0, 256},
       {RTS_TRAVERSAL_THREAD, 0, 1, 32},   {RTS_TRAVERSAL_THREAD, 0, 1, 128},
+      {RTS_TRAVERSAL_THREAD, 2, 1, 64},   {RTS_TRAVERSAL_THREAD, 2, 0, 64},
       {RTS_TRAVERSAL_THREAD, 4, 1, 64},   {RTS_TRAVERSAL_THREAD, 4, 1, 128},
       {RTS_TRAVERSAL_TEAM, 0, 1, 64},     {RTS_TRAVERSAL_TEAM, 4, 1, 128},
       {RTS_TRAVERSAL_FRONTIER, 4, 0, 64}, {RTS_TRAVERSAL_FRONTIER, 4, 1, 64},
+      {RTS_TRAVERSAL_PACKET, 0, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 64},
+      {RTS_TRAVERSAL_PACKET, 0, 1, 256},  {RTS_TRAVERSAL_PACKET, 4, 1, 256},
+      {RTS_TRAVERSAL_PACKET, 2, 1, 64},
   };
   double best = 1e300, first = -1;
   int best_w = ix->W;
