@@ -500,23 +500,27 @@ def run_query_bench(args, ctx):
                          "kernel": "rts::k_query (+ order sort when enabled)"},
             "cpu_baseline": cpu,
             "clocks": clocks_info,
-            "gpu_launches": args.steps * kernels_per_step(ix.config, nq, nbatch),
+            "gpu_launches": args.steps * kernels_per_step(ix.config, nq, nbatch, int(pred)),
         }
         print(json.dumps(line), flush=True)
     plan.close()
 
 
-def kernels_per_step(cfg, nq: int, nbatch: int) -> int:
+def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1) -> int:
     """Kernels of this library one batched launch runs: the query kernel, plus
     the order-key kernel and the radix sort's histogram, scan and one
-    onesweep pass per 8 key bits when queries are curve-sorted."""
+    onesweep pass per 8 key bits when queries are curve-sorted, plus the
+    query gather of a merged launch (several batches of one predicate that
+    count or use the packet scheme, sorted together on 32-bit keys)."""
     sorted_ = cfg.sort_queries == 1 or (cfg.sort_queries == 2 and nq >= 8192)
     if not sorted_:
         return 1
+    packet = cfg.traversal == 4 or (cfg.traversal == 0 and pred == 0)   # 0 = kIntersects
+    merged = nbatch > 1 and cfg.traversal not in (2, 3) and (handler == 0 or packet)
     end_bit = 32
-    while end_bit < 64 and (1 << (end_bit - 32)) < nbatch:
+    while not merged and end_bit < 64 and (1 << (end_bit - 32)) < nbatch:
         end_bit += 1
-    return 1 + 1 + 2 + (end_bit + 7) // 8
+    return 1 + 1 + 2 + (end_bit + 7) // 8 + (1 if merged else 0)
 
 
 def run_mutable_bench(args, ctx):

@@ -1,4 +1,4 @@
-// rtspatial::SpatialIndex<float, 2> on the B200 library.
+// rtspatial::SpatialIndex<float, 2> and <double, 2> on the B200 library.
 //
 // Same class, method names, argument types and asynchrony as the reference's
 // public API; every call forwards to the C-ABI in rtspatial_b200.h and throws
@@ -52,7 +52,7 @@ struct Config {
   uint32_t max_parallelism = 512;
   // B200 library knobs
   int handler = RTSPATIAL_DEFAULT_HANDLER;
-  int node_width = 8;
+  int node_width = 16;
   int traversal = RTS_TRAVERSAL_AUTO;
   int curve = RTS_CURVE_HILBERT;
   int max_trees = 8;
@@ -66,8 +66,10 @@ struct Config {
 
 template <typename COORD_T, int N_DIMS>
 class SpatialIndex {
-  static_assert(std::is_same<COORD_T, float>::value && N_DIMS == 2,
-                "the B200 library indexes float 2-D envelopes");
+  static_assert((std::is_same<COORD_T, float>::value || std::is_same<COORD_T, double>::value) &&
+                    N_DIMS == 2,
+                "the B200 library indexes float or double 2-D envelopes");
+  static constexpr bool kF64 = std::is_same<COORD_T, double>::value;
 
  public:
   using point_t = Point<COORD_T, N_DIMS>;
@@ -106,6 +108,7 @@ class SpatialIndex {
     c.sort_queries = config.sort_queries;
     c.query_occupancy = config.query_occupancy;
     c.frontier_factor = config.frontier_factor;
+    c.coord_bits = kF64 ? 64 : 32;
     if (h_) rts_destroy(h_);
     h_ = nullptr;
     RTS_CHECK(rts_create(&c, &h_));
@@ -114,8 +117,13 @@ class SpatialIndex {
   void Clear() { RTS_CHECK(rts_clear(handle(), nullptr)); }
 
   void Insert(ArrayView<envelope_t> envelopes, cudaStream_t stream = nullptr) {
-    RTS_CHECK(rts_insert(handle(), reinterpret_cast<const float*>(envelopes.data()),
-                         envelopes.size(), stream));
+    if constexpr (kF64) {
+      RTS_CHECK(rts_insert_f64(handle(), reinterpret_cast<const double*>(envelopes.data()),
+                               envelopes.size(), stream));
+    } else {
+      RTS_CHECK(rts_insert(handle(), reinterpret_cast<const float*>(envelopes.data()),
+                           envelopes.size(), stream));
+    }
   }
 
   void Delete(const ArrayView<size_t> ids, cudaStream_t stream) {
@@ -125,24 +133,44 @@ class SpatialIndex {
   }
 
   void Update(const ArrayView<thrust::pair<size_t, envelope_t>> updates, cudaStream_t stream) {
-    static_assert(sizeof(thrust::pair<size_t, envelope_t>) == sizeof(rts_update_entry),
-                  "update records are {size_t id; envelope}");
-    RTS_CHECK(rts_update(handle(), reinterpret_cast<const rts_update_entry*>(updates.data()),
-                         updates.size(), stream));
+    if constexpr (kF64) {
+      static_assert(sizeof(thrust::pair<size_t, envelope_t>) == sizeof(rts_update_entry_f64),
+                    "update records are {size_t id; envelope}");
+      RTS_CHECK(rts_update_f64(handle(),
+                               reinterpret_cast<const rts_update_entry_f64*>(updates.data()),
+                               updates.size(), stream));
+    } else {
+      static_assert(sizeof(thrust::pair<size_t, envelope_t>) == sizeof(rts_update_entry),
+                    "update records are {size_t id; envelope}");
+      RTS_CHECK(rts_update(handle(), reinterpret_cast<const rts_update_entry*>(updates.data()),
+                           updates.size(), stream));
+    }
   }
 
   void Query(Predicate p, ArrayView<point_t> queries, void* arg,
              cudaStream_t stream = nullptr) {
-    RTS_CHECK(rts_query_points(handle(), static_cast<int>(p),
-                               reinterpret_cast<const float*>(queries.data()), queries.size(),
-                               config_.handler, arg, stream));
+    if constexpr (kF64) {
+      RTS_CHECK(rts_query_points_f64(handle(), static_cast<int>(p),
+                                     reinterpret_cast<const double*>(queries.data()),
+                                     queries.size(), config_.handler, arg, stream));
+    } else {
+      RTS_CHECK(rts_query_points(handle(), static_cast<int>(p),
+                                 reinterpret_cast<const float*>(queries.data()), queries.size(),
+                                 config_.handler, arg, stream));
+    }
   }
 
   void Query(Predicate p, ArrayView<envelope_t> queries, void* arg,
              cudaStream_t stream = nullptr) {
-    RTS_CHECK(rts_query_envelopes(handle(), static_cast<int>(p),
-                                  reinterpret_cast<const float*>(queries.data()), queries.size(),
-                                  config_.handler, arg, stream));
+    if constexpr (kF64) {
+      RTS_CHECK(rts_query_envelopes_f64(handle(), static_cast<int>(p),
+                                        reinterpret_cast<const double*>(queries.data()),
+                                        queries.size(), config_.handler, arg, stream));
+    } else {
+      RTS_CHECK(rts_query_envelopes(handle(), static_cast<int>(p),
+                                    reinterpret_cast<const float*>(queries.data()),
+                                    queries.size(), config_.handler, arg, stream));
+    }
   }
 
   size_t size() const { return h_ ? rts_size(h_) : 0; }

@@ -82,6 +82,13 @@ typedef struct rts_update_entry {
   float min_x, min_y, max_x, max_y;
 } rts_update_entry;
 
+/* thrust::pair<size_t, Envelope<Point<double,2>>> for a double index
+ * (SpatialIndex<double, 2>, spatial_index.cuh:280-281). */
+typedef struct rts_update_entry_f64 {
+  uint64_t id;
+  double min_x, min_y, max_x, max_y;
+} rts_update_entry_f64;
+
 /* ---- configuration ---------------------------------------------------------
  * First block: the fields of rtspatial::Config (spatial_index.cuh:22-37),
  * accepted for source compatibility.  ptx_root has no counterpart (there are
@@ -102,7 +109,7 @@ typedef struct rts_config {
   uint32_t max_query_samples;      /* accepted, no effect */
   uint32_t max_parallelism;        /* accepted, no effect */
 
-  int32_t node_width;     /* children per node and boxes per leaf: 4, 8, 16 or 32 */
+  int32_t node_width;     /* children per node and boxes per leaf: 4, 8, 16 or 32 (default 16) */
   int32_t traversal;      /* RTS_TRAVERSAL_* */
   int32_t curve;          /* RTS_CURVE_*: the order leaves are packed in */
   int32_t max_trees;      /* insert batches kept as separate sub-trees before a merge rebuild (1..16) */
@@ -112,13 +119,17 @@ typedef struct rts_config {
   float rebuild_update_fraction; /* updates since the last rebuild, as a fraction of the index,
                                     above which Update re-sorts instead of refitting */
   uint32_t chunk;         /* queries per device work item (0 = library default) */
-  int32_t query_occupancy; /* 0 library default; 2 / 4: query kernel capped at 128 / 64
-                              registers (2 / 4 CTAs of 256 threads per SM) */
+  int32_t query_occupancy; /* 2 / 4: query kernel capped at 128 / 64 registers (2 / 4 CTAs
+                              of 256 threads per SM); 1: uncapped; 0: per scheme (thread 2,
+                              packet 4, team 1) */
   float frontier_factor;   /* frontier traversal: entries per query of each level buffer
                               (queries beyond it are answered depth-first); 0 = 16 */
+  int32_t coord_bits;      /* 32: SpatialIndex<float, 2>; 64: SpatialIndex<double, 2>, whose
+                              envelopes, points and updates go through the _f64 calls */
+  int32_t reserved;
 } rts_config;
 
-#define RTS_TRAVERSAL_AUTO 0
+#define RTS_TRAVERSAL_AUTO 0   /* packet for range-intersects launches, thread otherwise */
 #define RTS_TRAVERSAL_THREAD 1 /* one thread per query, loops over a node's children */
 #define RTS_TRAVERSAL_TEAM 2   /* node_width lanes per query, one child per lane */
 #define RTS_TRAVERSAL_FRONTIER 3 /* level by level over the whole launch (batches of one
@@ -164,6 +175,24 @@ int rts_update(rts_index* index, const rts_update_entry* updates, uint64_t n, vo
 int rts_query_points(rts_index* index, int predicate, const float* points, uint64_t n,
                      int handler, void* arg, void* stream);
 
+/* ---- double indexes (coord_bits = 64): SpatialIndex<double, 2> -------------
+ * The same calls over double envelopes {min.x, min.y, max.x, max.y}, points
+ * {x, y} and rts_update_entry_f64 (Insert, Update, Query of
+ * spatial_index.cuh:142-515 instantiated for double; rts_delete and the
+ * batched / planned / served calls apply unchanged, with the _F64 query
+ * kinds).  As in the reference, the contains predicates compare coordinates
+ * rounded to float (Point<double,2>::get_coordinate returns float,
+ * geom/point.cuh:68-71) while range-intersects runs the ray-slab test in
+ * double (details/ray_params.h:169-292).  A float index rejects these calls
+ * and a double index rejects the float ones (RTS_ERR_INVALID_ARGUMENT). */
+int rts_insert_f64(rts_index* index, const double* envelopes, uint64_t n, void* stream);
+int rts_update_f64(rts_index* index, const rts_update_entry_f64* updates, uint64_t n,
+                   void* stream);
+int rts_query_points_f64(rts_index* index, int predicate, const double* points, uint64_t n,
+                         int handler, void* arg, void* stream);
+int rts_query_envelopes_f64(rts_index* index, int predicate, const double* envelopes,
+                            uint64_t n, int handler, void* arg, void* stream);
+
 /* SpatialIndex::Query(Predicate, ArrayView<envelope_t>, void*, cudaStream_t)
  * (spatial_index.cuh:407-515): RTS_PREDICATE_CONTAINS reports boxes that
  * contain the query box; RTS_PREDICATE_INTERSECTS reports the reference's
@@ -181,6 +210,8 @@ int rts_query_envelopes(rts_index* index, int predicate, const float* envelopes,
  * batch's handler. */
 #define RTS_QUERY_POINTS 0
 #define RTS_QUERY_ENVELOPES 1
+#define RTS_QUERY_POINTS_F64 2    /* double index: 2 doubles per point */
+#define RTS_QUERY_ENVELOPES_F64 3 /* double index: 4 doubles per envelope */
 typedef struct rts_batch {
   int32_t query_kind; /* RTS_QUERY_POINTS or RTS_QUERY_ENVELOPES */
   int32_t predicate;  /* RTS_PREDICATE_* */
@@ -253,7 +284,8 @@ int rts_autotune(rts_index* index, const rts_batch* batches, uint32_t n_batches,
  * and estimated pairs.  Update requests (deletes, inserts, updates) apply
  * after every query submitted before them and before every later one.  A
  * request's pairs carry its own 0-based query ids and equal those of the same
- * query made alone on the index state it was submitted against. */
+ * query made alone on the index state it was submitted against.  A double
+ * index is served with the _F64 query kinds. */
 typedef struct rts_server rts_server;
 typedef struct rts_server_config {
   uint32_t slots;                  /* launches in flight (1..8) */
@@ -276,7 +308,8 @@ int rts_server_destroy(rts_server* server);
 int rts_server_submit_query(rts_server* server, int query_kind, int predicate,
                             const float* queries, uint64_t n, uint64_t* ticket);
 /* Copies an update batch: deletes, then updates, then inserts (new ids are
- * handed out in submission order; rts_server_take reports the first one). */
+ * handed out in submission order; rts_server_take reports the first one).
+ * A double index (coord_bits = 64) takes deletes only here. */
 int rts_server_submit_update(rts_server* server, const uint64_t* delete_ids, uint64_t n_delete,
                              const float* insert_envelopes, uint64_t n_insert,
                              const rts_update_entry* updates, uint64_t n_update,

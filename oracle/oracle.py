@@ -60,6 +60,18 @@ def _bind(lib: ctypes.CDLL, pfx: str) -> None:
     f.argtypes = [_vp, _vp, _u64]
 
 
+def _bind64(lib: ctypes.CDLL, pfx: str) -> None:
+    f = getattr(lib, pfx + "run")
+    f.restype = _u64
+    f.argtypes = [_vp, _u64, ctypes.c_int, _vp, _u64, _vp, _vp, _u64, ctypes.c_int]
+    f = getattr(lib, pfx + "eval_pairs")
+    f.restype = None
+    f.argtypes = [ctypes.c_int, _vp, _vp, _u64, _vp]
+    f = getattr(lib, pfx + "invalidate")
+    f.restype = None
+    f.argtypes = [_vp, _vp, _u64]
+
+
 def _ptr(a: np.ndarray | None) -> int | None:
     return None if a is None else a.ctypes.data
 
@@ -79,9 +91,12 @@ class Oracle:
         self.backend = backend
         self.lib = ctypes.CDLL(path)
         self.pfx = pfx
+        self.pfx64 = pfx.replace("ob_", "ob64_")
         _bind(self.lib, pfx)
+        _bind64(self.lib, self.pfx64)
         if backend == "port":
             self.lib.ob_port_slab_k.restype = ctypes.c_float
+            self.lib.ob64_port_slab_k.restype = ctypes.c_double
             for name, args in (
                 ("ob_fix_uniform_boxes", [_u64, ctypes.c_float, ctypes.c_float, _vp]),
                 ("ob_fix_uniform_points", [_u64, _vp]),
@@ -154,6 +169,44 @@ class Oracle:
         ids = np.ascontiguousarray(ids, dtype=np.uint64)
         assert boxes.dtype == np.float32 and boxes.flags.c_contiguous
         self._f("invalidate")(_ptr(boxes), _ptr(ids), ids.shape[0])
+
+    # -- double indexes (SpatialIndex<double, 2>), brute force --------------------
+    def run64(self, kind: int, boxes: np.ndarray, queries: np.ndarray, *,
+              collect: bool = True, threads: int | None = None):
+        """Same as ``run`` for float64 boxes and queries."""
+        boxes = np.ascontiguousarray(boxes, dtype=np.float64).reshape(-1, 4)
+        width = 2 if kind == KIND_POINT else 4
+        queries = np.ascontiguousarray(queries, dtype=np.float64).reshape(-1, width)
+        nb, nq = boxes.shape[0], queries.shape[0]
+        threads = threads or os.cpu_count() or 1
+        f = getattr(self.lib, self.pfx64 + "run")
+        counts = np.zeros(max(nq, 1), dtype=np.uint64)
+        total = int(f(_ptr(boxes), nb, kind, _ptr(queries), nq, _ptr(counts), None, 0, threads))
+        pairs = None
+        if collect:
+            pairs = np.zeros((max(total, 1), 2), dtype=np.uint32)
+            got = int(f(_ptr(boxes), nb, kind, _ptr(queries), nq, _ptr(counts), _ptr(pairs),
+                        total, threads))
+            assert got == total
+            pairs = pairs[:total]
+        return total, counts[:nq], pairs
+
+    def eval_pairs64(self, kind: int, g: np.ndarray, q: np.ndarray) -> np.ndarray:
+        g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1, 4)
+        width = 2 if kind == KIND_POINT else 4
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, width)
+        assert g.shape[0] == q.shape[0]
+        out = np.zeros(g.shape[0], dtype=np.uint8)
+        getattr(self.lib, self.pfx64 + "eval_pairs")(kind, _ptr(g), _ptr(q), g.shape[0], _ptr(out))
+        return out
+
+    def invalidate64(self, boxes: np.ndarray, ids) -> None:
+        ids = np.ascontiguousarray(ids, dtype=np.uint64)
+        assert boxes.dtype == np.float64 and boxes.flags.c_contiguous
+        getattr(self.lib, self.pfx64 + "invalidate")(_ptr(boxes), _ptr(ids), ids.shape[0])
+
+    def slab_k64(self) -> float:
+        return float(self.lib.ob64_port_slab_k())
 
     # -- fixtures (restated generator of the reference tests) ------------------
     def uniform_boxes(self, n: int, max_w: float, max_h: float) -> np.ndarray:

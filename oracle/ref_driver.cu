@@ -35,6 +35,35 @@ inline int ref_contains_box(const ob_box* g, const ob_box* q) {
   return to_env(g).Contains(to_env(q)) ? 1 : 0;
 }
 
+// SpatialIndex<double, 2>: Point<double,2>, Envelope<Point<double,2>> and
+// RayParams<double,2> (geom/point.cuh:44-75, details/ray_params.h:169-292).
+using ref_point64_t = rtspatial::Point<double, 2>;
+using ref_env64_t = rtspatial::Envelope<ref_point64_t>;
+
+inline ref_env64_t to_env64(const ob_box64* b) {
+  return ref_env64_t(ref_point64_t(b->minx, b->miny), ref_point64_t(b->maxx, b->maxy));
+}
+
+inline int ref_contains_point64(const ob_box64* g, double px, double py) {
+  return to_env64(g).Contains(ref_point64_t(px, py)) ? 1 : 0;
+}
+
+inline int ref_contains_box64(const ob_box64* g, const ob_box64* q) {
+  return to_env64(g).Contains(to_env64(q)) ? 1 : 0;
+}
+
+inline int ref_intersects64(const ob_box64* g, const ob_box64* q) {
+  ref_env64_t ge = to_env64(g), qe = to_env64(q);
+  rtspatial::details::RayParams<double, 2> rp;
+  rp.Compute(ge, false);
+  bool box_hit = rp.IsHit(qe);
+  bool backward = ge.IsValid() && box_hit;
+  rp.Compute(qe, true);
+  bool query_hit = rp.IsHit(ge);
+  bool forward = query_hit && !box_hit;
+  return (backward || forward) ? 1 : 0;
+}
+
 inline int ref_intersects(const ob_box* g, const ob_box* q) {
   ref_env_t ge = to_env(g), qe = to_env(q);
   rtspatial::details::RayParams<float, 2> rp;
@@ -79,3 +108,23 @@ void ob_ref_invalidate(ob_box* boxes, const uint64_t* ids, uint64_t n) {
   }
 }
 }
+
+extern "C" {
+#define OB64_PFX(name) ob64_ref_##name
+#define OB64_PRED_POINT(g, px, py) ref_contains_point64((g), (px), (py))
+#define OB64_PRED_CONTAINS(g, q) ref_contains_box64((g), (q))
+#define OB64_PRED_INTERSECTS(g, q) ref_intersects64((g), (q))
+#include "brute64_driver.h"
+
+/* Envelope<Point<double,2>>::Invalid() through the reference's own class. */
+void ob64_ref_invalidate(ob_box64* boxes, const uint64_t* ids, uint64_t n) {
+  for (uint64_t i = 0; i < n; i++) {
+    ref_env64_t e = to_env64(&boxes[ids[i]]);
+    e.Invalid();
+    boxes[ids[i]].minx = e.get_min().get_x();
+    boxes[ids[i]].miny = e.get_min().get_y();
+    boxes[ids[i]].maxx = e.get_max().get_x();
+    boxes[ids[i]].maxy = e.get_max().get_y();
+  }
+}
+}  // extern "C"

@@ -39,3 +39,18 @@ void ob_port_invalidate(ob_box* boxes, const uint64_t* ids, uint64_t n) {
   uint64_t i;
   for (i = 0; i < n; i++) ob_invalidate(&boxes[ids[i]]);
 }
+
+/* Double indexes: restated predicates behind the brute-force driver
+ * (exported prefix ob64_port_). */
+#define OB64_PFX(name) ob64_port_##name
+#define OB64_PRED_POINT(g, px, py) ob_contains_point64((g), (px), (py))
+#define OB64_PRED_CONTAINS(g, q) ob_contains_box64((g), (q))
+#define OB64_PRED_INTERSECTS(g, q) ob_intersects64((g), (q), ob_slab_k64())
+#include "brute64_driver.h"
+
+double ob64_port_slab_k(void) { return ob_slab_k64(); }
+
+void ob64_port_invalidate(ob_box64* boxes, const uint64_t* ids, uint64_t n) {
+  uint64_t i;
+  for (i = 0; i < n; i++) ob_invalidate64(&boxes[ids[i]]);
+}

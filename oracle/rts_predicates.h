@@ -124,4 +124,95 @@ static inline void ob_invalidate(ob_box* g) {
   g->maxy = g->miny;
 }
 
+/* ---- double-precision index (SpatialIndex<double, 2>) -------------------- */
+
+typedef struct {
+  double minx, miny, maxx, maxy;
+} ob_box64; /* layout of Envelope<Point<double,2>> */
+
+/* Point<double,2>::get_coordinate returns float (geom/point.cuh:68-71), and
+ * Envelope::Contains compares get_coordinate values (geom/envelope.cuh:29-53):
+ * a double index's contains predicates compare the coordinates rounded to the
+ * nearest float. */
+static inline int ob_contains_point64(const ob_box64* g, double px, double py) {
+  float x = (float)px, y = (float)py;
+  return x >= (float)g->minx && x <= (float)g->maxx && y >= (float)g->miny &&
+         y <= (float)g->maxy;
+}
+
+static inline int ob_contains_box64(const ob_box64* g, const ob_box64* q) {
+  return (float)q->minx >= (float)g->minx && (float)q->maxx <= (float)g->maxx &&
+         (float)q->miny >= (float)g->miny && (float)q->maxy <= (float)g->maxy;
+}
+
+/* Envelope::IsValid uses get_x/get_y, which return double
+ * (geom/envelope.cuh:103-105, geom/point.cuh:58-64). */
+static inline int ob_is_valid64(const ob_box64* g) {
+  return g->minx < g->maxx && g->miny < g->maxy;
+}
+
+/* 1 + 2 * DBL_GAMMA(3) evaluated in double (details/ray_params.h:41,283). */
+static inline double ob_slab_k64(void) {
+  volatile double three_eps = 3 * DBL_EPSILON;
+  volatile double gamma3 = three_eps / (1 - three_eps);
+  volatile double k = 1 + 2 * gamma3;
+  return k;
+}
+
+/* RayParams<double,2>::IsHit (details/ray_params.h:260-290): the slab test in
+ * double; its t1 start value is nextafterf(1.0, DBL_MAX), a float function,
+ * i.e. 1 + 2^-23 (OB_T1) widened to double. */
+static inline int ob_ray_hit64(double ox, double oy, double dx, double dy,
+                               const ob_box64* b, double k) {
+  double t0 = 0.0, t1 = (double)OB_T1;
+  double inv, tn, tf, tmp;
+
+  inv = 1.0 / dx;
+  tn = (b->minx - ox) * inv;
+  tf = (b->maxx - ox) * inv;
+  if (tn > tf) {
+    tmp = tn;
+    tn = tf;
+    tf = tmp;
+  }
+  tf = tf * k;
+  t0 = tn > t0 ? tn : t0;
+  t1 = tf < t1 ? tf : t1;
+  if (t0 > t1) return 0;
+
+  inv = 1.0 / dy;
+  tn = (b->miny - oy) * inv;
+  tf = (b->maxy - oy) * inv;
+  if (tn > tf) {
+    tmp = tn;
+    tn = tf;
+    tf = tmp;
+  }
+  tf = tf * k;
+  t0 = tn > t0 ? tn : t0;
+  t1 = tf < t1 ? tf : t1;
+  if (t0 > t1) return 0;
+  return 1;
+}
+
+/* Range-intersects result set of a double index: the same two-pass
+ * composition as ob_intersects (shaders_intersects_envelope_query_2d.cu
+ * compiled with FLOAT_TYPE = double), with RayParams<double,2>::Compute
+ * (details/ray_params.h:193-210) and IsHit in double. */
+static inline int ob_intersects64(const ob_box64* g, const ob_box64* q, double k) {
+  double gdx = g->maxx - g->minx;
+  double gdy = g->maxy - g->miny;
+  if (ob_ray_hit64(g->minx, g->miny, gdx, gdy, q, k)) return ob_is_valid64(g);
+  {
+    double qdx = q->minx - q->maxx;
+    double qdy = q->maxy - q->miny;
+    return ob_ray_hit64(q->maxx, q->miny, qdx, qdy, g, k);
+  }
+}
+
+static inline void ob_invalidate64(ob_box64* g) {
+  g->maxx = g->minx;
+  g->maxy = g->miny;
+}
+
 #endif /* RTS_ORACLE_PREDICATES_H */

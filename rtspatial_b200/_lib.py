@@ -34,6 +34,8 @@ RTS_CURVE_MORTON = 0
 RTS_CURVE_HILBERT = 1
 RTS_QUERY_POINTS = 0
 RTS_QUERY_ENVELOPES = 1
+RTS_QUERY_POINTS_F64 = 2
+RTS_QUERY_ENVELOPES_F64 = 3
 RTS_NOALLOC_MAX_BATCHES = 1024
 
 
@@ -61,6 +63,8 @@ class rts_config(ctypes.Structure):
         ("chunk", ctypes.c_uint32),
         ("query_occupancy", ctypes.c_int32),
         ("frontier_factor", ctypes.c_float),
+        ("coord_bits", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -71,6 +75,11 @@ class rts_queue(ctypes.Structure):
 class rts_update_entry(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint64), ("min_x", ctypes.c_float), ("min_y", ctypes.c_float),
                 ("max_x", ctypes.c_float), ("max_y", ctypes.c_float)]
+
+
+class rts_update_entry_f64(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("min_x", ctypes.c_double), ("min_y", ctypes.c_double),
+                ("max_x", ctypes.c_double), ("max_y", ctypes.c_double)]
 
 
 class rts_batch(ctypes.Structure):
@@ -121,6 +130,10 @@ SIGNATURES = {
     "rts_update": (_I, [_P, _P, _U64, _P]),
     "rts_query_points": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
     "rts_query_envelopes": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
+    "rts_insert_f64": (_I, [_P, _P, _U64, _P]),
+    "rts_update_f64": (_I, [_P, _P, _U64, _P]),
+    "rts_query_points_f64": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
+    "rts_query_envelopes_f64": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
     "rts_query_batched": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_query_batched_noalloc": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_plan_create": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, ctypes.POINTER(_P)]),

@@ -110,22 +110,26 @@ __global__ void k_curve_keys(const float4* __restrict__ boxes, const uint32_t* _
 __global__ void k_gather(const float4* __restrict__ src, const uint32_t* __restrict__ src_ids,
                          const uint32_t* __restrict__ order, uint64_t n, uint64_t id_begin,
                          uint64_t slot_base, float4* __restrict__ leaves,
-                         uint32_t* __restrict__ leaf_ids, uint32_t* __restrict__ pos) {
+                         uint32_t* __restrict__ leaf_ids, uint32_t* __restrict__ pos,
+                         const DBox* __restrict__ src64, DBox* __restrict__ leaves64) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t o = order[i];
   uint32_t id = src_ids ? src_ids[o] : static_cast<uint32_t>(id_begin + o);
   uint64_t slot = slot_base + i;
   leaves[slot] = src[o];
+  if (leaves64) leaves64[slot] = src64[o];
   leaf_ids[slot] = id;
   pos[id] = static_cast<uint32_t>(slot);
 }
 
 __global__ void k_fill_pad(float4* __restrict__ leaves, uint32_t* __restrict__ ids, uint64_t from,
-                           uint64_t to) {
+                           uint64_t to, DBox* __restrict__ leaves64) {
   uint64_t i = from + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= to) return;
   leaves[i] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+  if (leaves64)
+    leaves64[i] = DBox{make_double2(INFINITY, INFINITY), make_double2(-INFINITY, -INFINITY)};
   if (ids) ids[i] = 0xffffffffu;
 }
 
@@ -160,7 +164,8 @@ __global__ void k_slot_list(const uint64_t* __restrict__ meta, int n_trees,
 // Delete: Envelope::Invalid() (max := min) on each listed id below n_ids
 // (spatial_index.cuh:216-233); the box stays in its slot.
 __global__ void k_delete(const uint64_t* __restrict__ ids, uint64_t n, uint64_t n_ids,
-                         const uint32_t* __restrict__ pos, float4* __restrict__ leaves) {
+                         const uint32_t* __restrict__ pos, float4* __restrict__ leaves,
+                         DBox* __restrict__ leaves64) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint64_t id = ids[i];
@@ -170,6 +175,7 @@ __global__ void k_delete(const uint64_t* __restrict__ ids, uint64_t n, uint64_t 
   b.z = b.x;
   b.w = b.y;
   leaves[slot] = b;
+  if (leaves64) leaves64[slot].hi = leaves64[slot].lo;  // Invalid(): max := min in double
 }
 
 // Update: overwrite the envelope of each listed id (spatial_index.cuh:289-305).
@@ -180,6 +186,26 @@ __global__ void k_update(const rts_update_entry* __restrict__ upd, uint64_t n, u
   rts_update_entry e = upd[i];
   if (e.id >= n_ids) return;
   leaves[pos[e.id]] = make_float4(e.min_x, e.min_y, e.max_x, e.max_y);
+}
+
+// Double index: the double envelope and its float rounding.
+__global__ void k_update64(const rts_update_entry_f64* __restrict__ upd, uint64_t n,
+                           uint64_t n_ids, const uint32_t* __restrict__ pos,
+                           float4* __restrict__ leaves, DBox* __restrict__ leaves64) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  rts_update_entry_f64 e = upd[i];
+  if (e.id >= n_ids) return;
+  const DBox b{make_double2(e.min_x, e.min_y), make_double2(e.max_x, e.max_y)};
+  const uint32_t slot = pos[e.id];
+  leaves64[slot] = b;
+  leaves[slot] = round_box(b);
+}
+
+// Double index: float rounding of inserted envelopes.
+__global__ void k_round_boxes(const DBox* __restrict__ in, uint64_t n, float4* __restrict__ out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = round_box(in[i]);
 }
 
 __device__ __forceinline__ uint32_t batch_of_query(const BatchDesc* descs, uint32_t nb,
@@ -211,6 +237,11 @@ __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDes
   float2 c;
   if (B.pred == kPoint) {
     c = reinterpret_cast<const float2*>(B.queries)[local];
+  } else if (B.pred == kPoint64) {
+    const double2 p = reinterpret_cast<const double2*>(B.queries)[local];
+    c = make_float2(__double2float_rn(p.x), __double2float_rn(p.y));
+  } else if (B.pred >= kPoint64) {
+    c = center(round_box(reinterpret_cast<const DBox*>(B.queries)[local]));
   } else {
     c = center(reinterpret_cast<const float4*>(B.queries)[local]);
   }
@@ -222,6 +253,27 @@ __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDes
   uint32_t k = (curve == RTS_CURVE_HILBERT) ? hilbert16(qx, qy) : (spread16(qx) | (spread16(qy) << 1));
   keys[i] = merged ? k : (static_cast<unsigned long long>(b) << 32) | k;
   vals[i] = merged ? static_cast<uint32_t>(i) : local;
+}
+
+// Chunk visiting order of an unmerged sorted launch: chunk c of batch b
+// starts at sorted position qbase_b + (c - chunk_begin_b) * chunk, whose key
+// (batch << 32 | curve) gives the chunk's curve position.  Sorting chunks by
+// it makes the chunks in flight, whatever their batch, neighbours in space.
+__global__ void k_chunk_keys(const BatchDesc* __restrict__ descs, uint32_t nb,
+                             uint32_t total_chunks, uint32_t chunk,
+                             const unsigned long long* __restrict__ sorted_keys,
+                             uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (c >= total_chunks) return;
+  uint32_t lo = 0, hi = nb - 1;  // largest b with chunk_begin <= c
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (descs[mid].chunk_begin <= c) lo = mid; else hi = mid - 1;
+  }
+  const BatchDesc& B = descs[lo];
+  const uint64_t pos = B.qbase + static_cast<uint64_t>(c - B.chunk_begin) * chunk;
+  keys[c] = static_cast<uint32_t>(sorted_keys[pos]);
+  vals[c] = static_cast<uint32_t>(c);
 }
 
 // Merged launch: copies the queries in sorted order (order[j] = index in the
@@ -240,6 +292,10 @@ __global__ void k_merge_queries(const BatchDesc* __restrict__ descs, uint32_t nb
   const uint32_t local = g - B.qbase;
   if (B.pred == kPoint) {
     reinterpret_cast<float2*>(out_q)[j] = reinterpret_cast<const float2*>(B.queries)[local];
+  } else if (B.pred == kPoint64) {
+    reinterpret_cast<double2*>(out_q)[j] = reinterpret_cast<const double2*>(B.queries)[local];
+  } else if (B.pred >= kPoint64) {
+    reinterpret_cast<DBox*>(out_q)[j] = reinterpret_cast<const DBox*>(B.queries)[local];
   } else {
     reinterpret_cast<float4*>(out_q)[j] = reinterpret_cast<const float4*>(B.queries)[local];
   }
@@ -306,17 +362,18 @@ int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_
 
 int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
                   uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
-                  uint32_t* pos, cudaStream_t s) {
+                  uint32_t* pos, cudaStream_t s, const DBox* src64, DBox* leaves64) {
   if (n == 0) return RTS_OK;
   k_gather<<<grid_for(n), kThreads, 0, s>>>(src, src_ids, order, n, id_begin, slot_base, leaves,
-                                            leaf_ids, pos);
+                                            leaf_ids, pos, src64, leaves64);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }
 
-int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s) {
+int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s,
+                    DBox* leaves64) {
   if (to <= from) return RTS_OK;
-  k_fill_pad<<<grid_for(to - from), kThreads, 0, s>>>(leaves, ids, from, to);
+  k_fill_pad<<<grid_for(to - from), kThreads, 0, s>>>(leaves, ids, from, to, leaves64);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }
@@ -382,6 +439,32 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
   return RTS_OK;
 }
 
+int launch_chunk_order(const BatchDesc* descs, uint32_t nb, uint32_t total_chunks, uint32_t chunk,
+                       const unsigned long long* sorted_keys, uint32_t* keys_a, uint32_t* keys_b,
+                       uint32_t* vals_a, uint32_t* order, DevBuf& temp, cudaStream_t s) {
+  if (total_chunks == 0 || nb < 2) return RTS_OK;
+  k_chunk_keys<<<grid_for(total_chunks), kThreads, 0, s>>>(descs, nb, total_chunks, chunk,
+                                                           sorted_keys, keys_a, vals_a);
+  RTS_CUDA_TRY(cudaGetLastError());
+  size_t need = 0;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, keys_a, keys_b, vals_a, order,
+                                                static_cast<int>(total_chunks), 0, 32, s));
+  int rc = buf_reserve(temp, need, s, false, 0);
+  if (rc) return rc;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.ptr, need, keys_a, keys_b, vals_a, order,
+                                                static_cast<int>(total_chunks), 0, 32, s));
+  return RTS_OK;
+}
+
+int chunk_order_temp_bytes(uint32_t total_chunks, size_t* bytes) {
+  *bytes = 0;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(
+      nullptr, *bytes, static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+      static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+      static_cast<int>(total_chunks), 0, 32));
+  return RTS_OK;
+}
+
 int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes) {
   int end_bit = 32;
   while (end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
@@ -394,9 +477,9 @@ int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes) {
 }
 
 int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
-                  float4* leaves, cudaStream_t s) {
+                  float4* leaves, cudaStream_t s, DBox* leaves64) {
   if (n == 0) return RTS_OK;
-  k_delete<<<grid_for(n), kThreads, 0, s>>>(ids, n, n_ids, pos, leaves);
+  k_delete<<<grid_for(n), kThreads, 0, s>>>(ids, n, n_ids, pos, leaves, leaves64);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }
@@ -405,6 +488,21 @@ int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const
                   float4* leaves, cudaStream_t s) {
   if (n == 0) return RTS_OK;
   k_update<<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, leaves);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_update64(const rts_update_entry_f64* upd, uint64_t n, uint64_t n_ids,
+                    const uint32_t* pos, float4* leaves, DBox* leaves64, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_update64<<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, leaves, leaves64);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_round_boxes(const DBox* in, uint64_t n, float4* out, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_round_boxes<<<grid_for(n), kThreads, 0, s>>>(in, n, out);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }

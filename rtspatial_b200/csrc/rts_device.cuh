@@ -22,11 +22,29 @@ constexpr int kMaxLevels = 16;
 constexpr int kMaxTrees = 16;
 constexpr uint32_t kFull = 0xffffffffu;
 
-enum PredKind : int { kPoint = 0, kContains = 1, kIntersects = 2 };
+// The *64 kinds are the queries of a double index (SpatialIndex<double, 2>).
+enum PredKind : int {
+  kPoint = 0,
+  kContains = 1,
+  kIntersects = 2,
+  kPoint64 = 3,
+  kContains64 = 4,
+  kIntersects64 = 5
+};
+constexpr int kNumPreds = 6;
+
+// A double envelope {min.x, min.y, max.x, max.y} as two 16-byte halves.
+struct __align__(16) DBox {
+  double2 lo, hi;
+};
+__device__ __forceinline__ DBox load_dbox(const DBox* p) {
+  return DBox{__ldg(&p->lo), __ldg(&p->hi)};
+}
 enum HandlerKind : int { kCount = 0, kCollect = 1 };
 
 struct TreeDesc {
   const float4* leaves;  // first slot of this tree
+  const DBox* leaves64;  // double index: the double envelopes of the same slots
   const uint32_t* ids;   // leaf_ids of the first slot
   const float4* nodes;   // nodes[0] = root box; level L at nodes + level_off[L]
   uint32_t n;            // envelopes in this tree
@@ -180,6 +198,92 @@ __device__ __forceinline__ float2 root_magnitude(float4 r) {
 }
 
 // ---------------------------------------------------------------------------
+// Double index (SpatialIndex<double, 2>).  Its float leaves hold each double
+// envelope rounded to nearest, which is what Envelope::Contains compares
+// (Point<double,2>::get_coordinate returns float, geom/point.cuh:68-71), so
+// point- and range-contains run the float predicates on rounded queries.
+// Range-intersects runs RayParams<double,2>::IsHit in double.
+// ---------------------------------------------------------------------------
+
+// 1 + 2 * DBL_GAMMA(3) in double arithmetic = 1 + 6 * 2^-52
+// (details/ray_params.h:41,283).
+constexpr double kSlabK64 = 0x1.0000000000006p+0;
+
+__device__ __forceinline__ float4 round_box(DBox b) {
+  return make_float4(__double2float_rn(b.lo.x), __double2float_rn(b.lo.y),
+                     __double2float_rn(b.hi.x), __double2float_rn(b.hi.y));
+}
+
+// RayParams<double,2>::IsHit (details/ray_params.h:260-290); t1 starts at
+// nextafterf(1.0, DBL_MAX), a float value.
+__device__ __forceinline__ bool slab_hit64(double ox, double oy, double invx, double invy,
+                                           DBox b) {
+  double t0 = 0.0, t1 = static_cast<double>(kT1);
+  double tn = __dmul_rn(__dsub_rn(b.lo.x, ox), invx);
+  double tf = __dmul_rn(__dsub_rn(b.hi.x, ox), invx);
+  if (tn > tf) {
+    double t = tn;
+    tn = tf;
+    tf = t;
+  }
+  tf = __dmul_rn(tf, kSlabK64);
+  t0 = tn > t0 ? tn : t0;
+  t1 = tf < t1 ? tf : t1;
+  if (t0 > t1) return false;
+  tn = __dmul_rn(__dsub_rn(b.lo.y, oy), invy);
+  tf = __dmul_rn(__dsub_rn(b.hi.y, oy), invy);
+  if (tn > tf) {
+    double t = tn;
+    tn = tf;
+    tf = t;
+  }
+  tf = __dmul_rn(tf, kSlabK64);
+  t0 = tn > t0 ? tn : t0;
+  t1 = tf < t1 ? tf : t1;
+  return !(t0 > t1);
+}
+
+struct IsectQuery64 {
+  DBox q;               // the query envelope
+  double ox, oy;        // anti-diagonal ray origin (max.x, min.y)
+  double invx, invy;    // 1 / (min.x - max.x), 1 / (max.y - min.y)
+  float4 nb;            // float hull of q inflated by the node-test margin
+};
+
+__device__ __forceinline__ IsectQuery64 make_isect_query64(DBox q) {
+  IsectQuery64 Q;
+  Q.q = q;
+  // RayParams<double,2>::Compute(query, true) (details/ray_params.h:193-210).
+  Q.ox = q.hi.x;
+  Q.oy = q.lo.y;
+  Q.invx = __drcp_rn(__dsub_rn(q.lo.x, q.hi.x));
+  Q.invy = __drcp_rn(__dsub_rn(q.hi.y, q.lo.y));
+  Q.nb = make_float4(0.f, 0.f, 0.f, 0.f);
+  return Q;
+}
+
+// Node-test margin of the double predicate, on float hulls.  A pair accepted
+// by the double slab test has boxes at most (2^-23 + 2^-50)*|d| + 2^-50*M
+// apart (t1 = 1 + 2^-23); rounding both to float moves each bound by at most
+// 2^-24*M.  That is < 8*2^-24*M, far inside the margin 2^-17*M + 2^-120 of
+// isect_set_margin, applied to the rounded query.
+__device__ __forceinline__ void isect_set_margin64(IsectQuery64& Q, float2 mag) {
+  IsectQuery t;
+  t.q = round_box(Q.q);
+  isect_set_margin(t, mag);
+  Q.nb = t.nb;
+}
+
+// The double index's range-intersects result set: the composition of
+// isect_exact with RayParams<double,2> (Compute / IsHit in double).
+__device__ __forceinline__ bool isect_exact64(DBox g, const IsectQuery64& Q) {
+  double gix = __drcp_rn(__dsub_rn(g.hi.x, g.lo.x));
+  double giy = __drcp_rn(__dsub_rn(g.hi.y, g.lo.y));
+  if (slab_hit64(g.lo.x, g.lo.y, gix, giy, Q.q)) return g.lo.x < g.hi.x && g.lo.y < g.hi.y;
+  return slab_hit64(Q.ox, Q.oy, Q.invx, Q.invy, g);
+}
+
+// ---------------------------------------------------------------------------
 // Query adaptors: one per predicate, same interface.
 // ---------------------------------------------------------------------------
 template <int PRED>
@@ -193,6 +297,7 @@ template <>
 struct QueryOps<kPoint> {
   using Q = float2;
   static constexpr bool kRefine = false;
+  static constexpr bool kNeeds64 = false;
   static __device__ __forceinline__ bool coarse(float4 e, const Q& p) { return contains_point(e, p); }
   static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
     return reinterpret_cast<const float2*>(qs)[i];
@@ -206,6 +311,7 @@ template <>
 struct QueryOps<kContains> {
   using Q = float4;
   static constexpr bool kRefine = false;
+  static constexpr bool kNeeds64 = false;
   static __device__ __forceinline__ bool coarse(float4 e, const Q& q) { return contains_box(e, q); }
   static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
     return reinterpret_cast<const float4*>(qs)[i];
@@ -220,6 +326,7 @@ template <>
 struct QueryOps<kIntersects> {
   using Q = IsectQuery;
   static constexpr bool kRefine = true;
+  static constexpr bool kNeeds64 = false;
   static __device__ __forceinline__ bool coarse(float4 e, const Q& q) {
     return overlaps(make_float4(fminf(e.x, e.z), fminf(e.y, e.w), fmaxf(e.x, e.z), fmaxf(e.y, e.w)),
                     q.nb);
@@ -233,6 +340,44 @@ struct QueryOps<kIntersects> {
   }
   static __device__ __forceinline__ bool node(float4 e, const Q& q) { return overlaps(e, q.nb); }
   static __device__ __forceinline__ bool leaf(float4 g, const Q& q) { return isect_leaf(g, q); }
+};
+
+// Double index, contains predicates: the float operations on the query
+// rounded to nearest.
+template <>
+struct QueryOps<kPoint64> : QueryOps<kPoint> {
+  static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
+    const double2 p = reinterpret_cast<const double2*>(qs)[i];
+    return make_float2(__double2float_rn(p.x), __double2float_rn(p.y));
+  }
+};
+
+template <>
+struct QueryOps<kContains64> : QueryOps<kContains> {
+  static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
+    return round_box(reinterpret_cast<const DBox*>(qs)[i]);
+  }
+};
+
+// Double index, range-intersects: float hull tests (sound by the margin),
+// then the exact double predicate on the slot's double envelope (exact64).
+template <>
+struct QueryOps<kIntersects64> {
+  using Q = IsectQuery64;
+  static constexpr bool kRefine = true;
+  static constexpr bool kNeeds64 = true;
+  static __device__ __forceinline__ bool coarse(float4 e, const Q& q) {
+    return overlaps(make_float4(fminf(e.x, e.z), fminf(e.y, e.w), fmaxf(e.x, e.z), fmaxf(e.y, e.w)),
+                    q.nb);
+  }
+  static __device__ __forceinline__ bool exact64(DBox g, const Q& q) { return isect_exact64(g, q); }
+  static __device__ __forceinline__ Q load(const float* qs, uint32_t i) {
+    return make_isect_query64(reinterpret_cast<const DBox*>(qs)[i]);
+  }
+  static __device__ __forceinline__ void enter_tree(Q& q, float4 root) {
+    isect_set_margin64(q, root_magnitude(root));
+  }
+  static __device__ __forceinline__ bool node(float4 e, const Q& q) { return overlaps(e, q.nb); }
 };
 
 // ---------------------------------------------------------------------------

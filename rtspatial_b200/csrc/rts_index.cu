@@ -92,6 +92,9 @@ int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
   uint64_t need = slots + kSlotAlign;
   int rc = buf_reserve(ix->leaves, need * sizeof(float4), s, true, ix->slot_end * sizeof(float4));
   if (rc) return rc;
+  if (is_f64(ix) &&
+      (rc = buf_reserve(ix->leaves64, need * sizeof(DBox), s, true, ix->slot_end * sizeof(DBox))))
+    return rc;
   return buf_reserve(ix->leaf_ids, need * sizeof(uint32_t), s, true,
                      ix->slot_end * sizeof(uint32_t));
 }
@@ -115,6 +118,7 @@ float4* leaves_of(rts_index* ix) { return static_cast<float4*>(ix->leaves.ptr); 
 uint32_t* ids_of(rts_index* ix) { return static_cast<uint32_t*>(ix->leaf_ids.ptr); }
 uint32_t* pos_of(rts_index* ix) { return static_cast<uint32_t*>(ix->pos.ptr); }
 
+
 // Allocates the node buffer of `t` and packs its levels from its leaves.
 int build_tree_levels(rts_index* ix, HostTree& t, cudaStream_t s) {
   plan_levels(t.n, ix->W, t);
@@ -127,9 +131,11 @@ int build_tree_levels(rts_index* ix, HostTree& t, cudaStream_t s) {
 
 // Sorts `n` boxes (src[idx[i]] or src[i]) along the curve, writes them and
 // their ids to slots [slot_base, slot_base + n), and records pos[].
+// src64 / dst64: a double index's double envelopes, moved with their slots.
 int sort_into_slots(rts_index* ix, const float4* src, const uint32_t* src_ids, const uint32_t* idx,
                     uint64_t n, uint64_t id_begin, uint64_t slot_base, float4* dst_leaves,
-                    uint32_t* dst_ids, cudaStream_t s) {
+                    uint32_t* dst_ids, cudaStream_t s, const DBox* src64 = nullptr,
+                    DBox* dst64 = nullptr) {
   int rc = ensure_sort_scratch(ix, n, s);
   if (rc) return rc;
   auto* bounds = static_cast<uint32_t*>(ix->bounds.ptr);
@@ -141,9 +147,10 @@ int sort_into_slots(rts_index* ix, const float4* src, const uint32_t* src_ids, c
   if ((rc = launch_curve_keys(src, idx, n, bounds, ix->cfg.curve, ka, va, s))) return rc;
   if ((rc = sort_pairs(ka, kb, va, vb, n, ix->sort_temp, s))) return rc;
   if ((rc = launch_gather(src, src_ids, vb, n, id_begin, slot_base, dst_leaves, dst_ids,
-                          pos_of(ix), s)))
+                          pos_of(ix), s, src64, dst64)))
     return rc;
-  return launch_fill_pad(dst_leaves, dst_ids, slot_base + n, slot_base + round_up(n, kSlotAlign), s);
+  return launch_fill_pad(dst_leaves, dst_ids, slot_base + n, slot_base + round_up(n, kSlotAlign), s,
+                         dst64);
 }
 
 int rebuild_all_impl(rts_index* ix, cudaStream_t s);
@@ -187,25 +194,39 @@ int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
                              max_n, slots, s)))
     return rc;
   // New slot arrays; the old ones are read by the gather.
-  DevBuf new_leaves, new_ids;
+  DevBuf new_leaves, new_ids, new_leaves64;
   const uint64_t slots_needed = round_up(N, kSlotAlign);
+  auto drop = [&]() {
+    buf_free(new_leaves, s);
+    buf_free(new_ids, s);
+    buf_free(new_leaves64, s);
+  };
   if ((rc = buf_reserve(new_leaves, std::max(ix->leaves.bytes, (slots_needed + kSlotAlign) * sizeof(float4)), s, false, 0)))
     return rc;
   if ((rc = buf_reserve(new_ids, std::max(ix->leaf_ids.bytes, (slots_needed + kSlotAlign) * sizeof(uint32_t)), s, false, 0))) {
-    buf_free(new_leaves, s);
+    drop();
+    return rc;
+  }
+  if (is_f64(ix) &&
+      (rc = buf_reserve(new_leaves64, std::max(ix->leaves64.bytes, (slots_needed + kSlotAlign) * sizeof(DBox)), s, false, 0))) {
+    drop();
     return rc;
   }
   rc = sort_into_slots(ix, leaves_of(ix), ids_of(ix), slots, N, 0, 0,
-                       static_cast<float4*>(new_leaves.ptr), static_cast<uint32_t*>(new_ids.ptr), s);
+                       static_cast<float4*>(new_leaves.ptr), static_cast<uint32_t*>(new_ids.ptr), s,
+                       leaves64_of(ix), is_f64(ix) ? static_cast<DBox*>(new_leaves64.ptr) : nullptr);
   if (rc) {
-    buf_free(new_leaves, s);
-    buf_free(new_ids, s);
+    drop();
     return rc;
   }
   buf_free(ix->leaves, s);
   buf_free(ix->leaf_ids, s);
   ix->leaves = new_leaves;
   ix->leaf_ids = new_ids;
+  if (is_f64(ix)) {
+    buf_free(ix->leaves64, s);
+    ix->leaves64 = new_leaves64;
+  }
   for (auto& t : ix->trees) buf_free(t.nodes, s);
   ix->trees.clear();
   HostTree t;
@@ -232,6 +253,7 @@ void refresh_forest(rts_index* ix) {
     const HostTree& h = ix->trees[i];
     TreeDesc& d = F.tree[i];
     d.leaves = leaves_of(ix) + h.slot_base;
+    d.leaves64 = is_f64(ix) ? leaves64_of(ix) + h.slot_base : nullptr;
     d.ids = ids_of(ix) + h.slot_base;
     d.nodes = static_cast<const float4*>(h.nodes.ptr);
     d.n = static_cast<uint32_t>(h.n);
@@ -248,8 +270,14 @@ LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   LaunchPlan p;
   p.width = ix->W;
   int trav = ix->cfg.traversal;
-  if (trav == RTS_TRAVERSAL_AUTO) trav = RTS_TRAVERSAL_THREAD;
-  (void)pred;
+  // Default scheme, from B200 measurements: range-intersects walks its
+  // (sorted) queries in packets, the other predicates a query per lane.
+  if (trav == RTS_TRAVERSAL_AUTO)
+    trav = (pred == kIntersects || pred == kIntersects64) ? RTS_TRAVERSAL_PACKET
+                                                          : RTS_TRAVERSAL_THREAD;
+  // Double indexes run the thread or packet scheme only.
+  if (is_f64(ix) && (trav == RTS_TRAVERSAL_TEAM || trav == RTS_TRAVERSAL_FRONTIER))
+    trav = RTS_TRAVERSAL_THREAD;
   p.frontier = (trav == RTS_TRAVERSAL_FRONTIER);
   p.team = (trav == RTS_TRAVERSAL_TEAM);
   p.packet = (trav == RTS_TRAVERSAL_PACKET);
@@ -259,7 +287,8 @@ LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   const uint64_t warps = static_cast<uint64_t>(device_sm_count()) * 32;
   const uint64_t fair = ((total + 4 * warps - 1) / (4 * warps) + 31) / 32 * 32;
   p.chunk = static_cast<uint32_t>(std::max<uint64_t>(32, std::min<uint64_t>(chunk, fair)));
-  const int occ = ix->cfg.query_occupancy;
+  int occ = ix->cfg.query_occupancy;
+  if (occ == 0) occ = p.packet ? 4 : (p.team ? 1 : 2);  // library default per scheme
   p.min_blocks = occ >= 4 ? 4 : (occ >= 2 ? 2 : 1);
   return p;
 }
@@ -281,17 +310,29 @@ bool merge_batches(const LaunchPlan& plan, const BatchDesc* descs, uint32_t nd) 
 }
 
 int plan_order(QueryScratch& qs, const LaunchPlan& plan, BatchDesc* descs, uint32_t nd,
-               uint64_t total, cudaStream_t s) {
+               uint64_t total, uint64_t chunks, cudaStream_t s) {
   int rc;
   if ((rc = buf_reserve(qs.keys_a, total * 8, s, false, 0))) return rc;
   if ((rc = buf_reserve(qs.keys_b, total * 8, s, false, 0))) return rc;
   if ((rc = buf_reserve(qs.vals, total * 4, s, false, 0))) return rc;
   if ((rc = buf_reserve(qs.order, total * 4, s, false, 0))) return rc;
   if (plan.merged) {
-    if ((rc = buf_reserve(qs.m_queries, total * 16, s, false, 0))) return rc;
+    if ((rc = buf_reserve(qs.m_queries, total * sizeof(DBox), s, false, 0))) return rc;
     if ((rc = buf_reserve(qs.m_batch, total * 4, s, false, 0))) return rc;
     if ((rc = buf_reserve(qs.m_ident, total * 4, s, false, 0))) return rc;
     if ((rc = buf_reserve(qs.m_routes, nd * sizeof(DevQueue), s, false, 0))) return rc;
+  }
+  if (plan.chunk_order) {
+    const uint64_t b = std::max<uint64_t>(chunks, 1) * 4;
+    if ((rc = buf_reserve(qs.ck_keys_a, b, s, false, 0)) ||
+        (rc = buf_reserve(qs.ck_keys_b, b, s, false, 0)) ||
+        (rc = buf_reserve(qs.ck_vals, b, s, false, 0)) ||
+        (rc = buf_reserve(qs.ck_order, b, s, false, 0)))
+      return rc;
+    size_t need = 0;
+    if ((rc = chunk_order_temp_bytes(static_cast<uint32_t>(chunks), &need)) ||
+        (rc = buf_reserve(qs.sort_temp, need, s, false, 0)))
+      return rc;
   }
   uint64_t q = 0;
   for (uint32_t i = 0; i < nd; ++i) {
@@ -305,8 +346,8 @@ int plan_order(QueryScratch& qs, const LaunchPlan& plan, BatchDesc* descs, uint3
 // Fills the visiting order planned by plan_order (descriptors already on the
 // device when nd > 1).
 int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const BatchDesc* host,
-               const BatchDesc* dev, uint32_t nd, uint64_t total, cudaStream_t s) {
-  return launch_query_order(dev, host[0], nd, total,
+               const BatchDesc* dev, uint32_t nd, uint64_t total, uint64_t chunks, cudaStream_t s) {
+  int rc = launch_query_order(dev, host[0], nd, total,
                             static_cast<const float4*>(ix->trees[0].nodes.ptr), ix->cfg.curve,
                             static_cast<unsigned long long*>(qs.keys_a.ptr),
                             static_cast<unsigned long long*>(qs.keys_b.ptr),
@@ -316,6 +357,13 @@ int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
                             static_cast<uint32_t*>(qs.m_ident.ptr),
                             host[0].mode == kCollect ? static_cast<DevQueue*>(qs.m_routes.ptr)
                                                      : nullptr);
+  if (rc || !plan.chunk_order) return rc;
+  return launch_chunk_order(dev, nd, static_cast<uint32_t>(chunks), plan.chunk,
+                            static_cast<const unsigned long long*>(qs.keys_b.ptr),
+                            static_cast<uint32_t*>(qs.ck_keys_a.ptr),
+                            static_cast<uint32_t*>(qs.ck_keys_b.ptr),
+                            static_cast<uint32_t*>(qs.ck_vals.ptr),
+                            static_cast<uint32_t*>(qs.ck_order.ptr), qs.sort_temp, s);
 }
 
 // Turns public batch descriptions into launch descriptors (validating them);
@@ -327,22 +375,25 @@ int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches
   chunks = 0;
   uint64_t qsum = 0;
   int rc;
-  (void)ix;
   for (uint32_t i = 0; i < n_batches; ++i) {
     const rts_batch& b = batches[i];
     if ((rc = check_handler(b.handler, b.arg))) return rc;
     int pred;
-    if (b.query_kind == RTS_QUERY_POINTS) {
+    const bool f64 = b.query_kind == RTS_QUERY_POINTS_F64 || b.query_kind == RTS_QUERY_ENVELOPES_F64;
+    if (b.query_kind == RTS_QUERY_POINTS || b.query_kind == RTS_QUERY_POINTS_F64) {
       if (b.predicate != RTS_PREDICATE_CONTAINS)
         return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
-      pred = kPoint;
-    } else if (b.query_kind == RTS_QUERY_ENVELOPES) {
-      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
-      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
+      pred = f64 ? kPoint64 : kPoint;
+    } else if (b.query_kind == RTS_QUERY_ENVELOPES || b.query_kind == RTS_QUERY_ENVELOPES_F64) {
+      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = f64 ? kContains64 : kContains;
+      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = f64 ? kIntersects64 : kIntersects;
       else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
     } else {
       return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
     }
+    if (f64 != is_f64(ix))
+      return fail(RTS_ERR_INVALID_ARGUMENT, f64 ? "double queries on a float index"
+                                                : "float queries on a double index (use the _F64 kinds)");
     if (b.n == 0) continue;
     if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
     if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
@@ -415,7 +466,10 @@ int run_launch(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
                           s, nullptr, nullptr, &mo);
   }
   if (!uniform)
-    return launch_queries(ix->forest, plan, descs, dd, nd, static_cast<uint32_t>(chunks), work, s);
+    return launch_queries(ix->forest, plan, descs, dd, nd, static_cast<uint32_t>(chunks), work, s,
+                          nullptr, nullptr, nullptr,
+                          plan.chunk_order ? static_cast<const uint32_t*>(qs.ck_order.ptr)
+                                           : nullptr);
   int rc = reserve_frontier(ix, qs, total, s);
   if (rc) return rc;
   if ((rc = launch_frontier(ix->forest, descs[0].pred, descs[0].mode, descs, dd, nd,
@@ -425,6 +479,15 @@ int run_launch(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
   fallback.frontier = false;
   return launch_queries(ix->forest, fallback, descs, dd, nd, static_cast<uint32_t>(chunks), work, s,
                         qs.fb.spill, qs.fb.any_spill);
+}
+
+int launch_pred(const rts_batch* batches, uint32_t n) {
+  bool isect = n > 0;
+  for (uint32_t i = 0; i < n && isect; ++i)
+    isect = (batches[i].query_kind == RTS_QUERY_ENVELOPES ||
+             batches[i].query_kind == RTS_QUERY_ENVELOPES_F64) &&
+            batches[i].predicate == RTS_PREDICATE_INTERSECTS;
+  return isect ? kIntersects : kContains;
 }
 
 uint64_t sum_queries(const rts_batch* batches, uint32_t n) {
@@ -460,8 +523,9 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   b.qbase = 0;
   LaunchPlan plan = plan_for(ix, pred, n);
   if (want_sort(ix, n)) {
-    if ((rc = plan_order(ix->qs, plan, &b, 1, n, s))) return rc;
-    if ((rc = fill_order(ix, ix->qs, plan, &b, nullptr, 1, n, s))) return rc;
+    const uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
+    if ((rc = plan_order(ix->qs, plan, &b, 1, n, chunks, s))) return rc;
+    if ((rc = fill_order(ix, ix->qs, plan, &b, nullptr, 1, n, chunks, s))) return rc;
   }
   uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
   return run_launch(ix, ix->qs, plan, &b, nullptr, 1, n, chunks, s);
@@ -488,7 +552,7 @@ int rts_config_default(rts_config* c) {
   c->max_query_samples = 1000;
   c->max_parallelism = 512;
   // This library's structure defaults.
-  c->node_width = 8;
+  c->node_width = 16;
   c->traversal = RTS_TRAVERSAL_AUTO;
   c->curve = RTS_CURVE_HILBERT;
   c->max_trees = 8;
@@ -497,6 +561,7 @@ int rts_config_default(rts_config* c) {
   c->query_occupancy = 0;
   c->rebuild_update_fraction = 0.25f;
   c->chunk = 0;
+  c->coord_bits = 32;
   return RTS_OK;
 }
 
@@ -513,6 +578,9 @@ int rts_create(const rts_config* cfg, rts_index** out) {
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad curve");
   if (c.max_trees < 1 || c.max_trees > kMaxTrees)
     return fail(RTS_ERR_INVALID_ARGUMENT, "max_trees must be in 1..16");
+  if (c.coord_bits == 0) c.coord_bits = 32;
+  if (c.coord_bits != 32 && c.coord_bits != 64)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "coord_bits must be 32 or 64");
   auto* ix = new (std::nothrow) rts_index();
   if (!ix) return fail(RTS_ERR_OUT_OF_MEMORY, "host allocation failed");
   keep_pool_memory();
@@ -539,7 +607,8 @@ int rts_destroy(rts_index* ix) {
     buf_free(t.nodes, s);
   }
   DevBuf* all[] = {&ix->leaves, &ix->leaf_ids, &ix->pos, &ix->keys_a, &ix->keys_b, &ix->vals_a,
-                   &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp};
+                   &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp, &ix->leaves64,
+                   &ix->rounded};
   for (DevBuf* b : all) {
     touched |= b->ptr != nullptr;
     buf_free(*b, s);
@@ -567,21 +636,22 @@ int rts_clear(rts_index* ix, void* stream) {
   return RTS_OK;
 }
 
-int rts_insert(rts_index* ix, const float* envelopes, uint64_t n, void* stream) {
-  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
-  if (n == 0) return RTS_OK;  // spatial_index.cuh:144-146
-  if (!envelopes) return fail(RTS_ERR_INVALID_ARGUMENT, "envelopes is null");
+}  // extern "C"
+
+namespace rts {
+
+// Insert of n envelopes given as floats (src) and, for a double index, as
+// doubles (src64; src is then their float rounding).
+int insert_impl(rts_index* ix, const float4* src, const DBox* src64, uint64_t n, cudaStream_t s) {
   if (ix->n_ids + n >= 0xffffffffull)
     return fail(RTS_ERR_CAPACITY, "ids are 32-bit: at most 2^32-2 envelopes per index");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const auto* src = reinterpret_cast<const float4*>(envelopes);
   int rc;
   const uint64_t slot_base = ix->slot_end;
   const uint64_t slot_end = slot_base + round_up(n, kSlotAlign);
   if ((rc = ensure_slots(ix, slot_end, s))) return rc;
   if ((rc = ensure_ids(ix, ix->n_ids + n, s))) return rc;
   if ((rc = sort_into_slots(ix, src, nullptr, nullptr, n, ix->n_ids, slot_base, leaves_of(ix),
-                            ids_of(ix), s)))
+                            ids_of(ix), s, src64, leaves64_of(ix))))
     return rc;
   HostTree t;
   t.id_begin = ix->n_ids;
@@ -603,33 +673,88 @@ int rts_insert(rts_index* ix, const float* envelopes, uint64_t n, void* stream) 
   return RTS_OK;
 }
 
-int rts_delete(rts_index* ix, const uint64_t* ids, uint64_t n, void* stream) {
-  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
-  if (n == 0 || ix->n_ids == 0) return RTS_OK;
-  if (!ids) return fail(RTS_ERR_INVALID_ARGUMENT, "ids is null");
-  return launch_delete(ids, n, ix->n_ids, pos_of(ix), leaves_of(ix),
-                       static_cast<cudaStream_t>(stream));
-}
-
-int rts_update(rts_index* ix, const rts_update_entry* upd, uint64_t n, void* stream) {
-  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
-  if (n == 0 || ix->n_ids == 0) return RTS_OK;
-  if (!upd) return fail(RTS_ERR_INVALID_ARGUMENT, "updates is null");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int rc = launch_update(upd, n, ix->n_ids, pos_of(ix), leaves_of(ix), s);
-  if (rc) return rc;
+// After n envelopes were overwritten: refit every sub-tree, or re-sort once
+// the updates since the last build pass the configured fraction.
+int after_update(rts_index* ix, uint64_t n, cudaStream_t s) {
   ix->updated_since_build += n;
   if (static_cast<double>(ix->updated_since_build) >
       ix->cfg.rebuild_update_fraction * static_cast<double>(ix->n_ids))
     return rebuild_all(ix, s);
+  int rc;
   for (auto& t : ix->trees)
     if ((rc = launch_pack_tree(leaves_of(ix) + t.slot_base, t, ix->W, s))) return rc;
   return RTS_OK;
 }
 
+int check_coords(const rts_index* ix, bool f64) {
+  if (f64 == is_f64(ix)) return RTS_OK;
+  return fail(RTS_ERR_INVALID_ARGUMENT, f64 ? "double call on a float index (coord_bits = 32)"
+                                            : "float call on a double index (use the _f64 calls)");
+}
+
+}  // namespace rts
+
+extern "C" {
+
+int rts_insert(rts_index* ix, const float* envelopes, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  int rc = check_coords(ix, false);
+  if (rc) return rc;
+  if (n == 0) return RTS_OK;  // spatial_index.cuh:144-146
+  if (!envelopes) return fail(RTS_ERR_INVALID_ARGUMENT, "envelopes is null");
+  return insert_impl(ix, reinterpret_cast<const float4*>(envelopes), nullptr, n,
+                     static_cast<cudaStream_t>(stream));
+}
+
+int rts_insert_f64(rts_index* ix, const double* envelopes, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  int rc = check_coords(ix, true);
+  if (rc) return rc;
+  if (n == 0) return RTS_OK;
+  if (!envelopes) return fail(RTS_ERR_INVALID_ARGUMENT, "envelopes is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const auto* src64 = reinterpret_cast<const DBox*>(envelopes);
+  if ((rc = buf_reserve(ix->rounded, n * sizeof(float4), s, false, 0))) return rc;
+  auto* rounded = static_cast<float4*>(ix->rounded.ptr);
+  if ((rc = launch_round_boxes(src64, n, rounded, s))) return rc;
+  return insert_impl(ix, rounded, src64, n, s);
+}
+
+int rts_delete(rts_index* ix, const uint64_t* ids, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (n == 0 || ix->n_ids == 0) return RTS_OK;
+  if (!ids) return fail(RTS_ERR_INVALID_ARGUMENT, "ids is null");
+  return launch_delete(ids, n, ix->n_ids, pos_of(ix), leaves_of(ix),
+                       static_cast<cudaStream_t>(stream), leaves64_of(ix));
+}
+
+int rts_update(rts_index* ix, const rts_update_entry* upd, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  int rc = check_coords(ix, false);
+  if (rc) return rc;
+  if (n == 0 || ix->n_ids == 0) return RTS_OK;
+  if (!upd) return fail(RTS_ERR_INVALID_ARGUMENT, "updates is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if ((rc = launch_update(upd, n, ix->n_ids, pos_of(ix), leaves_of(ix), s))) return rc;
+  return after_update(ix, n, s);
+}
+
+int rts_update_f64(rts_index* ix, const rts_update_entry_f64* upd, uint64_t n, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  int rc = check_coords(ix, true);
+  if (rc) return rc;
+  if (n == 0 || ix->n_ids == 0) return RTS_OK;
+  if (!upd) return fail(RTS_ERR_INVALID_ARGUMENT, "updates is null");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if ((rc = launch_update64(upd, n, ix->n_ids, pos_of(ix), leaves_of(ix), leaves64_of(ix), s)))
+    return rc;
+  return after_update(ix, n, s);
+}
+
 int rts_query_points(rts_index* ix, int predicate, const float* points, uint64_t n, int handler,
                      void* arg, void* stream) {
   if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (int rc = check_coords(ix, false)) return rc;
   if (predicate != RTS_PREDICATE_CONTAINS)
     return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
   return query_one(ix, kPoint, points, n, handler, arg, static_cast<cudaStream_t>(stream));
@@ -638,6 +763,7 @@ int rts_query_points(rts_index* ix, int predicate, const float* points, uint64_t
 int rts_query_envelopes(rts_index* ix, int predicate, const float* envelopes, uint64_t n,
                         int handler, void* arg, void* stream) {
   if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (int rc = check_coords(ix, false)) return rc;
   int pred;
   if (predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
   else if (predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
@@ -645,12 +771,34 @@ int rts_query_envelopes(rts_index* ix, int predicate, const float* envelopes, ui
   return query_one(ix, pred, envelopes, n, handler, arg, static_cast<cudaStream_t>(stream));
 }
 
+int rts_query_points_f64(rts_index* ix, int predicate, const double* points, uint64_t n,
+                         int handler, void* arg, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (int rc = check_coords(ix, true)) return rc;
+  if (predicate != RTS_PREDICATE_CONTAINS)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
+  return query_one(ix, kPoint64, reinterpret_cast<const float*>(points), n, handler, arg,
+                   static_cast<cudaStream_t>(stream));
+}
+
+int rts_query_envelopes_f64(rts_index* ix, int predicate, const double* envelopes, uint64_t n,
+                            int handler, void* arg, void* stream) {
+  if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
+  if (int rc = check_coords(ix, true)) return rc;
+  int pred;
+  if (predicate == RTS_PREDICATE_CONTAINS) pred = kContains64;
+  else if (predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects64;
+  else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
+  return query_one(ix, pred, reinterpret_cast<const float*>(envelopes), n, handler, arg,
+                   static_cast<cudaStream_t>(stream));
+}
+
 int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batches, void* stream) {
   if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
   if (n_batches == 0) return RTS_OK;
   if (!batches) return fail(RTS_ERR_INVALID_ARGUMENT, "batches is null");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  LaunchPlan plan = plan_for(ix, kContains, sum_queries(batches, n_batches));
+  LaunchPlan plan = plan_for(ix, launch_pred(batches, n_batches), sum_queries(batches, n_batches));
   std::vector<BatchDesc> descs;
   uint64_t chunks = 0;
   int rc = make_descs(ix, batches, n_batches, plan, descs, chunks);
@@ -662,15 +810,16 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   for (const auto& d : descs) total += d.n;
   const bool sorted = want_sort(ix, total);
   plan.merged = sorted && merge_batches(plan, descs.data(), static_cast<uint32_t>(descs.size()));
+  plan.chunk_order = sorted && !plan.merged && !plan.frontier && descs.size() > 1;
   if (sorted && (rc = plan_order(ix->qs, plan, descs.data(), static_cast<uint32_t>(descs.size()),
-                                 total, s)))
+                                 total, chunks, s)))
     return rc;
   void* ddev = nullptr;
   if (descs.size() > 1 &&
       (rc = ix->staging.put(descs.data(), descs.size() * sizeof(BatchDesc), s, &ddev)))
     return rc;
   if (sorted && (rc = fill_order(ix, ix->qs, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
-                                 static_cast<uint32_t>(descs.size()), total, s)))
+                                 static_cast<uint32_t>(descs.size()), total, chunks, s)))
     return rc;
   return run_launch(ix, ix->qs, plan, descs.data(), static_cast<const BatchDesc*>(ddev),
                     static_cast<uint32_t>(descs.size()), total, chunks, s);
@@ -717,7 +866,7 @@ uint32_t rts_num_trees(const rts_index* ix) {
 
 uint64_t rts_memory_usage(const rts_index* ix) {
   if (!ix) return 0;
-  uint64_t b = ix->leaves.bytes + ix->leaf_ids.bytes + ix->pos.bytes;
+  uint64_t b = ix->leaves.bytes + ix->leaf_ids.bytes + ix->pos.bytes + ix->leaves64.bytes;
   for (const auto& t : ix->trees) b += t.nodes.bytes;
   return b;
 }

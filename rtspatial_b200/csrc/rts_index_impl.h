@@ -66,12 +66,14 @@ struct QueryScratch {
   DevBuf work, keys_a, keys_b, vals, order, sort_temp;
   // merged launch: queries in sorted order, their batch and reported id
   DevBuf m_queries, m_batch, m_ident, m_routes;
+  // unmerged sorted launch: chunk keys and the chunk visiting order
+  DevBuf ck_keys_a, ck_keys_b, ck_vals, ck_order;
   // frontier traversal
   DevBuf fr_qbuf, fr_qaux, fr_qbatch, fr_vis, fr_a, fr_b, fr_counts, fr_spill, fr_any;
   FrontierBufs fb;
   void release(cudaStream_t s) {
     DevBuf* all[] = {&work, &keys_a, &keys_b, &vals, &order, &sort_temp, &m_queries, &m_batch,
-                     &m_ident, &m_routes, &fr_qbuf, &fr_qaux, &fr_qbatch, &fr_vis, &fr_a, &fr_b,
+                     &m_ident, &m_routes, &ck_keys_a, &ck_keys_b, &ck_vals, &ck_order, &fr_qbuf, &fr_qaux, &fr_qbatch, &fr_vis, &fr_a, &fr_b,
                      &fr_counts, &fr_spill, &fr_any};
     for (DevBuf* b : all) buf_free(*b, s);
   }
@@ -89,6 +91,8 @@ struct rts_index {
   uint64_t updated_since_build = 0;
   uint64_t version = 0;         // bumped when buffers or sub-trees change
   rts::DevBuf leaves, leaf_ids, pos;
+  rts::DevBuf leaves64;         // double index: the double envelopes, slot by slot
+  rts::DevBuf rounded;          // double index: scratch of an insert's float rounding
   std::vector<rts::HostTree> trees;
   // scratch of the build path
   rts::DevBuf keys_a, keys_b, vals_a, vals_b, sort_temp, bounds, slots_tmp;
@@ -110,12 +114,20 @@ struct rts_index {
 namespace rts {
 
 inline uint64_t round_up(uint64_t a, uint64_t b) { return (a + b - 1) / b * b; }
+inline bool is_f64(const rts_index* ix) { return ix->cfg.coord_bits == 64; }
+// The double envelopes of a double index, slot by slot (nullptr otherwise).
+inline DBox* leaves64_of(rts_index* ix) {
+  return is_f64(ix) ? static_cast<DBox*>(ix->leaves64.ptr) : nullptr;
+}
 
 void refresh_forest(rts_index* ix);
 // Re-sorts every box of the index into one tree at the index's node width.
 int rebuild_all(rts_index* ix, cudaStream_t s);
 LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total_queries);
 uint64_t sum_queries(const rts_batch* batches, uint32_t n);
+// kIntersects when every batch is a range-intersects batch, else kContains
+// (the predicate plan_for picks the default traversal scheme by).
+int launch_pred(const rts_batch* batches, uint32_t n);
 void keep_pool_memory();
 bool want_sort(const rts_index* ix, uint64_t total);
 int check_handler(int handler, void* arg);
@@ -127,9 +139,9 @@ bool merge_batches(const LaunchPlan& plan, const BatchDesc* descs, uint32_t nd);
 // assigns each batch its slice of the launch's visiting order.  Call before
 // the descriptors are staged.
 int plan_order(QueryScratch& qs, const LaunchPlan& plan, BatchDesc* descs, uint32_t nd,
-               uint64_t total, cudaStream_t s);
+               uint64_t total, uint64_t chunks, cudaStream_t s);
 int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const BatchDesc* host,
-               const BatchDesc* dev, uint32_t nd, uint64_t total, cudaStream_t s);
+               const BatchDesc* dev, uint32_t nd, uint64_t total, uint64_t chunks, cudaStream_t s);
 int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
                const LaunchPlan& plan, std::vector<BatchDesc>& out, uint64_t& chunks);
 // Sizes the frontier buffers of `qs` for `total` queries (no-op when large

@@ -59,12 +59,14 @@ int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_
                uint64_t n, DevBuf& temp, cudaStream_t s);
 // For i < n with o = order[i]: leaves[slot_base+i] = src[o];
 // id = src_ids ? src_ids[o] : id_begin + o; leaf_ids[slot_base+i] = id;
-// pos[id] = slot_base + i.
+// pos[id] = slot_base + i.  A double index also gathers src64 into leaves64.
 int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
                   uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
-                  uint32_t* pos, cudaStream_t s);
+                  uint32_t* pos, cudaStream_t s, const DBox* src64 = nullptr,
+                  DBox* leaves64 = nullptr);
 // Empty boxes (+inf, +inf, -inf, -inf) in slots [from, to); ids = ~0.
-int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s);
+int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s,
+                    DBox* leaves64 = nullptr);
 // Levels 1..top and the root box of a tree from its leaves (also the refit).
 int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_t s);
 // slots[id_begin_t + i] = slot_base_t + i for every tree t; meta (device) =
@@ -83,13 +85,24 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
                        DevBuf& temp, cudaStream_t s, bool merged = false, void* merged_q = nullptr,
                        uint32_t* merged_batch = nullptr, uint32_t* merged_ident = nullptr,
                        DevQueue* merged_routes = nullptr);
+// Chunk visiting order of a sorted, unmerged launch of nb >= 2 batches:
+// order = chunk ids sorted by the curve key of each chunk's first query
+// (sorted_keys = the sorted query keys the order sort left in keys_b).
+int launch_chunk_order(const BatchDesc* descs, uint32_t nb, uint32_t total_chunks, uint32_t chunk,
+                       const unsigned long long* sorted_keys, uint32_t* keys_a, uint32_t* keys_b,
+                       uint32_t* vals_a, uint32_t* order, DevBuf& temp, cudaStream_t s);
+int chunk_order_temp_bytes(uint32_t total_chunks, size_t* bytes);
 // Temporary bytes the order sort of `total` queries in `nb` batches needs
 // (an upper bound for the merged sort too).
 int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes);
 int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
-                  float4* leaves, cudaStream_t s);
+                  float4* leaves, cudaStream_t s, DBox* leaves64 = nullptr);
 int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
                   float4* leaves, cudaStream_t s);
+int launch_update64(const rts_update_entry_f64* upd, uint64_t n, uint64_t n_ids,
+                    const uint32_t* pos, float4* leaves, DBox* leaves64, cudaStream_t s);
+// out[i] = the double envelope in[i] rounded to nearest float.
+int launch_round_boxes(const DBox* in, uint64_t n, float4* out, cudaStream_t s);
 
 // ---- frontier traversal (rts_frontier.cu) ---------------------------------
 struct FrontierBufs {
@@ -122,6 +135,7 @@ struct LaunchPlan {
   uint32_t chunk = 32;  // queries per work item
   int min_blocks = 1;         // CTAs of 256 threads per SM the registers are capped for (1, 2, 4)
   bool merged = false;        // sort the queries of all batches together (MergedOrder)
+  bool chunk_order = false;   // sorted, unmerged, several batches: chunks visited by space
 };
 // Runs `nb` batches (descriptors in host memory `hb`; device copy `db` when
 // nb > 1) in one persistent launch.  work_counter: zeroed device uint32.
@@ -130,7 +144,8 @@ struct LaunchPlan {
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
                    uint32_t* work_counter, cudaStream_t s, const uint32_t* only = nullptr,
-                   const uint32_t* only_any = nullptr, const MergedOrder* merged = nullptr);
+                   const uint32_t* only_any = nullptr, const MergedOrder* merged = nullptr,
+                   const uint32_t* chunk_order = nullptr);
 // Sets the chosen query kernel's shared-memory limit on the current device
 // (once; call outside stream capture before a launch is captured).
 int prepare_query_kernel(const LaunchPlan& plan);

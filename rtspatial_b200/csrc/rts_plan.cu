@@ -42,7 +42,7 @@ int enqueue(rts_plan* p, cudaStream_t s) {
   const BatchDesc* dd = static_cast<const BatchDesc*>(p->ddescs.ptr);
   int rc;
   if (p->sorted && (rc = fill_order(ix, p->qs, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd,
-                                    p->total, s)))
+                                    p->total, p->chunks, s)))
     return rc;
   return run_launch(ix, p->qs, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd, p->total,
                     p->chunks, s);
@@ -63,7 +63,8 @@ int rts_plan_create(rts_index* ix, const rts_batch* batches, uint32_t n_batches,
   auto* p = new (std::nothrow) rts_plan();
   if (!p) return fail(RTS_ERR_OUT_OF_MEMORY, "host allocation failed");
   p->ix = ix;
-  p->plan = plan_for(ix, kContains, n_batches ? sum_queries(batches, n_batches) : 0);
+  p->plan = plan_for(ix, launch_pred(batches, n_batches),
+                     n_batches ? sum_queries(batches, n_batches) : 0);
   int rc = make_descs(ix, batches, n_batches, p->plan, p->descs, p->chunks);
   cudaStream_t s = 0;
   for (const auto& d : p->descs) p->total += d.n;
@@ -72,8 +73,9 @@ int rts_plan_create(rts_index* ix, const rts_batch* batches, uint32_t n_batches,
   if (!rc && p->sorted) {
     p->plan.merged =
         merge_batches(p->plan, p->descs.data(), static_cast<uint32_t>(p->descs.size()));
+    p->plan.chunk_order = !p->plan.merged && !p->plan.frontier && p->descs.size() > 1;
     rc = plan_order(p->qs, p->plan, p->descs.data(), static_cast<uint32_t>(p->descs.size()),
-                    p->total, s);
+                    p->total, p->chunks, s);
     size_t need = 0;
     if (!rc) rc = query_order_temp_bytes(p->total, static_cast<uint32_t>(p->descs.size()), &need);
     if (!rc) rc = buf_reserve(p->qs.sort_temp, need, s, false, 0);

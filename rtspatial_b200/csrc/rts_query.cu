@@ -38,7 +38,19 @@ __device__ __noinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B,
     case kContains * 2 + kCollect: RTS_RUN(kContains, kCollect); break;
     case kIntersects * 2 + kCount: RTS_RUN(kIntersects, kCount); break;
     case kIntersects * 2 + kCollect: RTS_RUN(kIntersects, kCollect); break;
-    default: break;
+    default:
+      if constexpr (!TEAM) {  // double indexes (the team scheme is float only)
+        switch (B.pred * 2 + B.mode) {
+          case kPoint64 * 2 + kCount: RTS_RUN(kPoint64, kCount); break;
+          case kPoint64 * 2 + kCollect: RTS_RUN(kPoint64, kCollect); break;
+          case kContains64 * 2 + kCount: RTS_RUN(kContains64, kCount); break;
+          case kContains64 * 2 + kCollect: RTS_RUN(kContains64, kCollect); break;
+          case kIntersects64 * 2 + kCount: RTS_RUN(kIntersects64, kCount); break;
+          case kIntersects64 * 2 + kCollect: RTS_RUN(kIntersects64, kCollect); break;
+          default: break;
+        }
+      }
+      break;
   }
 #undef RTS_RUN
 }
@@ -51,7 +63,8 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     k_query(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
             const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
             uint32_t chunk, uint32_t* __restrict__ work, const uint32_t* __restrict__ only,
-            const uint32_t* __restrict__ only_any, const __grid_constant__ MergedOrder M) {
+            const uint32_t* __restrict__ only_any, const __grid_constant__ MergedOrder M,
+            const uint32_t* __restrict__ chunk_order) {
   if (only_any && *only_any == 0) return;
   __shared__ Forest F;
   __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
@@ -68,6 +81,7 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     if (lane == 0) c = atomicAdd(work, 1u);
     c = __shfl_sync(kFull, c, 0);
     if (c >= total_chunks) break;
+    if (chunk_order) c = __ldg(chunk_order + c);  // c < total_chunks: a permutation
     BatchDesc B;
     if (nb == 1) {
       B = b0;
@@ -99,6 +113,12 @@ __device__ __noinline__ void dispatch_packet(const Forest& F, const BatchDesc& B
     case kContains * 2 + kCollect: RTS_RUN(kContains, kCollect); break;
     case kIntersects * 2 + kCount: RTS_RUN(kIntersects, kCount); break;
     case kIntersects * 2 + kCollect: RTS_RUN(kIntersects, kCollect); break;
+    case kPoint64 * 2 + kCount: RTS_RUN(kPoint64, kCount); break;
+    case kPoint64 * 2 + kCollect: RTS_RUN(kPoint64, kCollect); break;
+    case kContains64 * 2 + kCount: RTS_RUN(kContains64, kCount); break;
+    case kContains64 * 2 + kCollect: RTS_RUN(kContains64, kCollect); break;
+    case kIntersects64 * 2 + kCount: RTS_RUN(kIntersects64, kCount); break;
+    case kIntersects64 * 2 + kCollect: RTS_RUN(kIntersects64, kCollect); break;
     default: break;
   }
 #undef RTS_RUN
@@ -117,7 +137,8 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     k_query_packet(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
                    const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
                    uint32_t chunk, uint32_t* __restrict__ work, const uint32_t* __restrict__,
-                   const uint32_t* __restrict__, const __grid_constant__ MergedOrder M) {
+                   const uint32_t* __restrict__, const __grid_constant__ MergedOrder M,
+                   const uint32_t* __restrict__ chunk_order) {
   __shared__ Forest F;
   __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
   // packet_stride<W>() per warp, then (merged launch) the warps' batch tables
@@ -135,6 +156,7 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
     if (lane == 0) c = atomicAdd(work, 1u);
     c = __shfl_sync(kFull, c, 0);
     if (c >= total_chunks) break;
+    if (chunk_order) c = __ldg(chunk_order + c);  // c < total_chunks: a permutation
     BatchDesc B;
     if (nb == 1) {
       B = b0;
@@ -159,7 +181,7 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
 
 using QueryKernel = void (*)(const Forest, const BatchDesc, const BatchDesc*, uint32_t, uint32_t,
                              uint32_t, uint32_t*, const uint32_t*, const uint32_t*,
-                             const MergedOrder);
+                             const MergedOrder, const uint32_t*);
 
 template <int MINB, bool ROUTED>
 static QueryKernel pick_kernel_occ(const LaunchPlan& p) {
@@ -265,7 +287,8 @@ int query_grid_size(const LaunchPlan& plan, uint32_t total_chunks, bool merged) 
 int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const BatchDesc* db, uint32_t nb, uint32_t total_chunks,
                    uint32_t* work_counter, cudaStream_t s, const uint32_t* only,
-                   const uint32_t* only_any, const MergedOrder* merged) {
+                   const uint32_t* only_any, const MergedOrder* merged,
+                   const uint32_t* chunk_order) {
   if (total_chunks == 0) return RTS_OK;
   LaunchPlan use = plan;
   if (only) use.packet = false;  // the packet scheme takes no query filter
@@ -278,7 +301,7 @@ int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
   RTS_CUDA_TRY(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), s));
   const MergedOrder M = merged ? *merged : MergedOrder{nullptr, nullptr, nullptr, nullptr};
   k<<<grid, kQueryThreads, dyn, s>>>(F, hb[0], db, nb, total_chunks, plan.chunk, work_counter,
-                                     only, only_any, M);
+                                     only, only_any, M, chunk_order);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }

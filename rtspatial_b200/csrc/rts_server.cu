@@ -173,7 +173,7 @@ struct rts_server {
   uint64_t next_ticket = 1;
   bool stop = false;
   std::thread worker;
-  double rate[3] = {4.0, 4.0, 4.0};  // pairs per query estimate per predicate
+  double rate[kNumPreds] = {4.0, 4.0, 4.0, 4.0, 4.0, 4.0};  // pairs per query, per PredKind
   // statistics
   std::vector<double> lat;
   uint64_t queries_done = 0, pairs_done = 0, launches = 0, retried = 0, updates_done = 0;
@@ -356,7 +356,7 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
   }
   int rc = RTS_OK;
   const bool sorted = want_sort(ix, total);
-  if (sorted) rc = plan_order(sl.qs, plan, sl.h_descs, np, total, s);
+  if (sorted) rc = plan_order(sl.qs, plan, sl.h_descs, np, total, chunks, s);
   cudaError_t e = cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, in_used, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(sl.d_queues.ptr, sl.h_queues, np * sizeof(DevQueue), cudaMemcpyHostToDevice, s);
@@ -366,7 +366,8 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
   if (e != cudaSuccess) rc = cuda_fail(e, "server launch staging");
   refresh_forest(ix);
   const BatchDesc* dd = static_cast<const BatchDesc*>(sl.d_descs.ptr);
-  if (!rc && sorted) rc = fill_order(ix, sl.qs, plan, sl.h_descs, np > 1 ? dd : nullptr, np, total, s);
+  if (!rc && sorted)
+    rc = fill_order(ix, sl.qs, plan, sl.h_descs, np > 1 ? dd : nullptr, np, total, chunks, s);
   if (!rc)
     rc = launch_queries(ix->forest, plan, sl.h_descs, np > 1 ? dd : nullptr, np,
                         static_cast<uint32_t>(chunks), static_cast<uint32_t*>(sl.qs.work.ptr), s);
@@ -641,25 +642,32 @@ int rts_server_submit_query(rts_server* sv, int query_kind, int predicate, const
   if (!sv || !ticket) return fail(RTS_ERR_INVALID_ARGUMENT, "server or ticket is null");
   if (n && !queries) return fail(RTS_ERR_INVALID_ARGUMENT, "queries is null");
   int pred;
-  uint32_t w;
-  if (query_kind == RTS_QUERY_POINTS && predicate == RTS_PREDICATE_CONTAINS) {
-    pred = kPoint;
-    w = 2;
-  } else if (query_kind == RTS_QUERY_ENVELOPES && predicate == RTS_PREDICATE_CONTAINS) {
-    pred = kContains;
-    w = 4;
-  } else if (query_kind == RTS_QUERY_ENVELOPES && predicate == RTS_PREDICATE_INTERSECTS) {
-    pred = kIntersects;
-    w = 4;
+  uint32_t w;  // 4-byte words per query (a double counts as two)
+  const bool f64 = query_kind == RTS_QUERY_POINTS_F64 || query_kind == RTS_QUERY_ENVELOPES_F64;
+  const bool points = query_kind == RTS_QUERY_POINTS || query_kind == RTS_QUERY_POINTS_F64;
+  const bool boxes = query_kind == RTS_QUERY_ENVELOPES || query_kind == RTS_QUERY_ENVELOPES_F64;
+  if (points && predicate == RTS_PREDICATE_CONTAINS) {
+    pred = f64 ? kPoint64 : kPoint;
+    w = f64 ? 4 : 2;
+  } else if (boxes && predicate == RTS_PREDICATE_CONTAINS) {
+    pred = f64 ? kContains64 : kContains;
+    w = f64 ? 8 : 4;
+  } else if (boxes && predicate == RTS_PREDICATE_INTERSECTS) {
+    pred = f64 ? kIntersects64 : kIntersects;
+    w = f64 ? 8 : 4;
   } else {
     return fail(RTS_ERR_INVALID_ARGUMENT, "unsupported query kind / predicate");
   }
+  if (f64 != is_f64(sv->ix))
+    return fail(RTS_ERR_INVALID_ARGUMENT, f64 ? "double queries on a float index"
+                                              : "float queries on a double index");
   if (n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a request");
   auto r = std::make_unique<Request>();
   r->pred = pred;
   r->qwidth = w;
   r->n = n;
-  r->q.assign(queries, queries + n * w);
+  r->q.resize(n * w);
+  if (n) std::memcpy(r->q.data(), queries, n * w * sizeof(float));
   r->t_submit = now_s();
   std::lock_guard<std::mutex> lock(sv->mu);
   if (sv->fatal) return fail(sv->fatal, "server stopped after an error");
@@ -684,6 +692,9 @@ int rts_server_submit_update(rts_server* sv, const uint64_t* delete_ids, uint64_
   if (!sv || !ticket) return fail(RTS_ERR_INVALID_ARGUMENT, "server or ticket is null");
   if ((n_delete && !delete_ids) || (n_insert && !insert_envelopes) || (n_update && !updates))
     return fail(RTS_ERR_INVALID_ARGUMENT, "null update array");
+  if (is_f64(sv->ix) && (n_insert || n_update))
+    return fail(RTS_ERR_INVALID_ARGUMENT,
+                "a served double index takes deletes only; insert and update it before serving");
   auto r = std::make_unique<Request>();
   r->is_update = true;
   r->del.assign(delete_ids, delete_ids + n_delete);

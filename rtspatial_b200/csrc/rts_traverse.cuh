@@ -136,7 +136,12 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       for (int c = 0; c < W; ++c)
         if (static_cast<uint32_t>(c) < lim && Ops::coarse(e[c], s.q)) m |= 1u << c;
       if (at_leaf) {
-        if constexpr (Ops::kRefine) {
+        if constexpr (Ops::kNeeds64) {  // exact test on the slots' double envelopes
+          const DBox* p64 = T.leaves64 + first;
+#pragma unroll
+          for (int c = 0; c < W; ++c)
+            if (((m >> c) & 1u) && !Ops::exact64(load_dbox(p64 + c), s.q)) m &= ~(1u << c);
+        } else if constexpr (Ops::kRefine) {
 #pragma unroll
           for (int c = 0; c < W; ++c)
             if (((m >> c) & 1u) && !Ops::exact(e[c], s.q)) m &= ~(1u << c);
@@ -172,7 +177,8 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
 }
 
 // ---------------------------------------------------------------------------
-// team scheme: W lanes per query, 32 / W queries in flight per warp
+// team scheme: W lanes per query, 32 / W queries in flight per warp (float
+// indexes only: double launches use the thread or packet scheme)
 // ---------------------------------------------------------------------------
 template <int PRED, int MODE, int W>
 __device__ __forceinline__ void run_chunk_team(const Forest& F, const BatchDesc& B,
@@ -278,11 +284,11 @@ constexpr int kSlices = 8;
 
 template <int W>
 constexpr size_t packet_smem_bytes() {
-  return sizeof(PacketSmem<kIntersects, W>) > sizeof(PacketSmem<kPoint, W>)
-             ? (sizeof(PacketSmem<kIntersects, W>) > sizeof(PacketSmem<kContains, W>)
-                    ? sizeof(PacketSmem<kIntersects, W>)
-                    : sizeof(PacketSmem<kContains, W>))
-             : sizeof(PacketSmem<kPoint, W>);
+  size_t m = sizeof(PacketSmem<kPoint, W>);
+  m = sizeof(PacketSmem<kContains, W>) > m ? sizeof(PacketSmem<kContains, W>) : m;
+  m = sizeof(PacketSmem<kIntersects, W>) > m ? sizeof(PacketSmem<kIntersects, W>) : m;
+  m = sizeof(PacketSmem<kIntersects64, W>) > m ? sizeof(PacketSmem<kIntersects64, W>) : m;
+  return m;
 }
 
 template <int PRED, int MODE, int W, bool ROUTED>
@@ -341,6 +347,8 @@ __device__ __forceinline__ void run_chunk_packet(const Forest& F, const BatchDes
         const bool valid = c < lim;
         uint32_t hm = 0;
         uint32_t rm = qm;
+        DBox g64{};          // double index: this entry's double envelope, loaded
+        bool have64 = false;  // the first time a query passes the float test
         while (rm) {  // uniform: kGroups queries per round
           uint32_t mine = rm;
 #pragma unroll
@@ -350,7 +358,19 @@ __device__ __forceinline__ void run_chunk_packet(const Forest& F, const BatchDes
           for (uint32_t k = 0; k < kGroups; ++k) rm &= rm - 1;
           if (mine && valid) {
             const uint32_t j = __ffs(mine) - 1;
-            const bool hit = at_leaf ? Ops::leaf(e, P.q[j]) : Ops::node(e, P.q[j]);
+            bool hit;
+            if constexpr (Ops::kNeeds64) {
+              hit = at_leaf ? Ops::coarse(e, P.q[j]) : Ops::node(e, P.q[j]);
+              if (hit && at_leaf) {
+                if (!have64) {
+                  g64 = load_dbox(T.leaves64 + first + c);
+                  have64 = true;
+                }
+                hit = Ops::exact64(g64, P.q[j]);
+              }
+            } else {
+              hit = at_leaf ? Ops::leaf(e, P.q[j]) : Ops::node(e, P.q[j]);
+            }
             if (hit) hm |= 1u << j;
           }
         }

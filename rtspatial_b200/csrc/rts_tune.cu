@@ -128,18 +128,19 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
   std::vector<int> widths;
   if (tune_width) widths = {4, 8, 16, 32};
   else widths = {ix->W};
+  // occupancy 1 = uncapped registers, 2 / 4 = capped for 2 / 4 CTAs per SM
   const Candidate cands[] = {
-      {RTS_TRAVERSAL_THREAD, 0, 0, 32},   {RTS_TRAVERSAL_THREAD, 0, 0, 128},
+      {RTS_TRAVERSAL_THREAD, 1, 0, 32},   {RTS_TRAVERSAL_THREAD, 1, 0, 128},
       {RTS_TRAVERSAL_THREAD, 4, 0, 32},   {RTS_TRAVERSAL_THREAD, 4, 0, 64},
       {RTS_TRAVERSAL_THREAD, 4, 0, 128},  {RTS_TRAVERSAL_THREAD, 4, 0, 256},
-      {RTS_TRAVERSAL_THREAD, 0, 1, 32},   {RTS_TRAVERSAL_THREAD, 0, 1, 128},
+      {RTS_TRAVERSAL_THREAD, 1, 1, 32},   {RTS_TRAVERSAL_THREAD, 1, 1, 128},
       {RTS_TRAVERSAL_THREAD, 2, 1, 64},   {RTS_TRAVERSAL_THREAD, 2, 0, 64},
+      {RTS_TRAVERSAL_THREAD, 2, 1, 128},  {RTS_TRAVERSAL_THREAD, 2, 0, 128},
       {RTS_TRAVERSAL_THREAD, 4, 1, 64},   {RTS_TRAVERSAL_THREAD, 4, 1, 128},
-      {RTS_TRAVERSAL_TEAM, 0, 1, 64},     {RTS_TRAVERSAL_TEAM, 4, 1, 128},
+      {RTS_TRAVERSAL_TEAM, 1, 1, 64},     {RTS_TRAVERSAL_TEAM, 4, 1, 128},
       {RTS_TRAVERSAL_FRONTIER, 4, 0, 64}, {RTS_TRAVERSAL_FRONTIER, 4, 1, 64},
-      {RTS_TRAVERSAL_PACKET, 0, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 64},
-      {RTS_TRAVERSAL_PACKET, 0, 1, 256},  {RTS_TRAVERSAL_PACKET, 4, 1, 256},
-      {RTS_TRAVERSAL_PACKET, 2, 1, 64},
+      {RTS_TRAVERSAL_PACKET, 1, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 64},
+      {RTS_TRAVERSAL_PACKET, 2, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 256},
   };
   double best = 1e300, first = -1;
   int best_w = ix->W;

@@ -28,9 +28,15 @@ class Server:
         check(lib().rts_server_create(index._handle(), ctypes.byref(c), ctypes.byref(self._h)))
 
     def submit(self, predicate, queries: np.ndarray) -> int:
-        q = np.ascontiguousarray(queries, dtype=np.float32)
-        kind = L.RTS_QUERY_POINTS if q.ndim == 2 and q.shape[1] == 2 else L.RTS_QUERY_ENVELOPES
-        n = q.shape[0] if q.ndim == 2 else q.size // (2 if kind == L.RTS_QUERY_POINTS else 4)
+        """Queues a query request; float64 arrays go to a double index."""
+        f64 = np.asarray(queries).dtype == np.float64
+        q = np.ascontiguousarray(queries, dtype=np.float64 if f64 else np.float32)
+        pts = q.ndim == 2 and q.shape[1] == 2
+        if f64:
+            kind = L.RTS_QUERY_POINTS_F64 if pts else L.RTS_QUERY_ENVELOPES_F64
+        else:
+            kind = L.RTS_QUERY_POINTS if pts else L.RTS_QUERY_ENVELOPES
+        n = q.shape[0] if q.ndim == 2 else q.size // (2 if pts else 4)
         t = ctypes.c_uint64()
         check(lib().rts_server_submit_query(self._h, kind, int(predicate), q.ctypes.data, n,
                                             ctypes.byref(t)))

@@ -71,7 +71,7 @@ class Config:
     max_query_samples: int = 1000
     max_parallelism: int = 512
     # structure / traversal
-    node_width: int = 8
+    node_width: int = 16
     traversal: int = L.RTS_TRAVERSAL_AUTO
     curve: int = L.RTS_CURVE_HILBERT
     max_trees: int = 8
@@ -81,6 +81,7 @@ class Config:
     chunk: int = 0
     query_occupancy: int = 0
     frontier_factor: float = 0.0
+    coord_bits: int = 32    # 64: SpatialIndex<double, 2> (float64 tensors throughout)
 
     def to_c(self) -> L.rts_config:
         c = L.rts_config()
@@ -101,11 +102,11 @@ def _stream_handle(stream) -> int | None:
     return stream.cuda_stream
 
 
-def _f32(t: torch.Tensor, width: int, name: str) -> torch.Tensor:
+def _f32(t: torch.Tensor, width: int, name: str, dtype=torch.float32) -> torch.Tensor:
     if not isinstance(t, torch.Tensor) or not t.is_cuda:
         raise TypeError(f"{name} must be a CUDA tensor")
-    if t.dtype != torch.float32:
-        raise TypeError(f"{name} must be float32")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {str(dtype).replace('torch.', '')}")
     t = t.reshape(-1, width)
     if not t.is_contiguous():
         t = t.contiguous()
@@ -218,9 +219,18 @@ class SpatialIndex:
         check(lib().rts_clear(self._handle(), _stream_handle(stream)))
 
     # -- mutation ---------------------------------------------------------------
+    @property
+    def _f64(self) -> bool:
+        return self.config.coord_bits == 64
+
+    @property
+    def _dtype(self):
+        return torch.float64 if self._f64 else torch.float32
+
     def Insert(self, envelopes: torch.Tensor, stream=None) -> None:
-        e = _f32(envelopes, 4, "envelopes")
-        check(lib().rts_insert(self._handle(), e.data_ptr(), e.shape[0], _stream_handle(stream)))
+        e = _f32(envelopes, 4, "envelopes", self._dtype)
+        fn = lib().rts_insert_f64 if self._f64 else lib().rts_insert
+        check(fn(self._handle(), e.data_ptr(), e.shape[0], _stream_handle(stream)))
         self._keep = e  # the copy is asynchronous
 
     def Delete(self, ids: torch.Tensor, stream=None) -> None:
@@ -234,27 +244,28 @@ class SpatialIndex:
         """Overwrites envelopes[i] at id ids[i] (the reference takes
         ``thrust::pair<size_t, envelope_t>``; this packs the same 24-byte
         records)."""
-        e = _f32(envelopes, 4, "envelopes")
+        e = _f32(envelopes, 4, "envelopes", self._dtype)
         ids = ids.to(device=e.device, dtype=torch.int64).reshape(-1, 1)
         if ids.shape[0] != e.shape[0]:
             raise ValueError("ids and envelopes differ in length")
-        rec = torch.cat([ids, e.view(torch.int64)], dim=1).contiguous()
-        check(lib().rts_update(self._handle(), rec.data_ptr(), rec.shape[0], _stream_handle(stream)))
+        rec = torch.cat([ids, e.view(torch.int64)], dim=1).contiguous()   # 24 or 40 bytes
+        fn = lib().rts_update_f64 if self._f64 else lib().rts_update
+        check(fn(self._handle(), rec.data_ptr(), rec.shape[0], _stream_handle(stream)))
         self._keep = rec
 
     # -- queries ------------------------------------------------------------------
     def Query(self, predicate: Predicate, queries: torch.Tensor, arg: int, stream=None,
               handler: Handler = Handler.COLLECT) -> None:
         """Reference-shaped query: results go to the handler's ``arg``."""
+        f64 = self._f64
         if queries.dim() == 2 and queries.shape[1] == 2:
-            q = _f32(queries, 2, "queries")
-            check(lib().rts_query_points(self._handle(), int(predicate), q.data_ptr(), q.shape[0],
-                                         int(handler), arg, _stream_handle(stream)))
+            q = _f32(queries, 2, "queries", self._dtype)
+            fn = lib().rts_query_points_f64 if f64 else lib().rts_query_points
         else:
-            q = _f32(queries, 4, "queries")
-            check(lib().rts_query_envelopes(self._handle(), int(predicate), q.data_ptr(),
-                                            q.shape[0], int(handler), arg,
-                                            _stream_handle(stream)))
+            q = _f32(queries, 4, "queries", self._dtype)
+            fn = lib().rts_query_envelopes_f64 if f64 else lib().rts_query_envelopes
+        check(fn(self._handle(), int(predicate), q.data_ptr(), q.shape[0], int(handler), arg,
+                 _stream_handle(stream)))
 
     def query_count(self, predicate: Predicate, queries: torch.Tensor, stream=None) -> int:
         c = Counter(queries.device)
@@ -326,9 +337,13 @@ def _batch_array(batches):
     keep = []
     for i, (pred, q, handler, arg) in enumerate(batches):
         is_pt = q.dim() == 2 and q.shape[1] == 2
-        q = _f32(q, 2 if is_pt else 4, "queries")
+        f64 = q.dtype == torch.float64
+        q = _f32(q, 2 if is_pt else 4, "queries", torch.float64 if f64 else torch.float32)
         keep.append(q)
-        arr[i].query_kind = L.RTS_QUERY_POINTS if is_pt else L.RTS_QUERY_ENVELOPES
+        if f64:
+            arr[i].query_kind = L.RTS_QUERY_POINTS_F64 if is_pt else L.RTS_QUERY_ENVELOPES_F64
+        else:
+            arr[i].query_kind = L.RTS_QUERY_POINTS if is_pt else L.RTS_QUERY_ENVELOPES
         arr[i].predicate = int(pred)
         arr[i].queries = q.data_ptr()
         arr[i].n = q.shape[0]

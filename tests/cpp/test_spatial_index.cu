@@ -262,6 +262,37 @@ TEST_CASE(CollectingQueue, matches_count) {
   EXPECT_EQ_OR_FAIL(static_cast<unsigned long long>(seen.size()), n);
 }
 
+// SpatialIndex<double, 2> (test_commons.h:12's spatial_index_d2d_t): the
+// point KAT's float inputs widened to double give the same count, since the
+// double index's contains compares float-rounded coordinates.
+TEST_CASE(PointQueries, fp64_contains_point_large_batch) {
+  using dindex_t = SpatialIndex<double, 2>;
+  using dpoint_t = dindex_t::point_t;
+  using denvelope_t = dindex_t::envelope_t;
+  std::vector<envelope_t> envf = uniform_boxes(100000, 0.5, 0.5);
+  std::vector<point_t> qf = uniform_points(1000);
+  std::vector<denvelope_t> envd(envf.size());
+  std::vector<dpoint_t> qd(qf.size());
+  for (size_t i = 0; i < envf.size(); ++i)
+    envd[i] = denvelope_t(dpoint_t(envf[i].get_min().get_x(), envf[i].get_min().get_y()),
+                          dpoint_t(envf[i].get_max().get_x(), envf[i].get_max().get_y()));
+  for (size_t i = 0; i < qf.size(); ++i) qd[i] = dpoint_t(qf[i].get_x(), qf[i].get_y());
+  thrust::device_vector<denvelope_t> env = envd;
+  thrust::device_vector<dpoint_t> q = qd;
+  Stream s;
+  Config config;
+  dindex_t index;
+  index.Init(config);
+  size_t avg = (env.size() + 9) / 10;
+  for (size_t b = 0; b < env.size(); b += avg)
+    index.Insert(ArrayView<denvelope_t>(thrust::raw_pointer_cast(env.data()) + b,
+                                        std::min(avg, env.size() - b)),
+                 s.cuda_stream());
+  counter().set(s.cuda_stream(), 0);
+  index.Query(Predicate::kContains, ArrayView<dpoint_t>(q), counter().data(), s.cuda_stream());
+  EXPECT_EQ_OR_FAIL(counter().get(s.cuda_stream()), 4224111ull);
+}
+
 }  // namespace
 
 int main() {

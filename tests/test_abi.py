@@ -18,7 +18,7 @@ HEADER = os.path.join(ROOT, "include", "rtspatial_b200.h")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(rts_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(rts_[a-z0-9_]+)\s*\(", src)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -41,6 +41,8 @@ int main(void) {
          sizeof(rts_update_entry), sizeof(rts_batch));
   printf("%zu %zu %zu %zu\n", offsetof(rts_update_entry, min_x), offsetof(rts_queue, size),
          offsetof(rts_batch, arg), offsetof(rts_config, chunk));
+  printf("%zu %zu %zu\n", sizeof(rts_update_entry_f64), offsetof(rts_update_entry_f64, min_x),
+         offsetof(rts_config, coord_bits));
   return 0;
 }
 ''')
@@ -57,6 +59,9 @@ int main(void) {
     assert sizes[1] == 24 and sizes[6] == 16
     assert sizes[7] == L.rts_batch.arg.offset
     assert sizes[8] == L.rts_config.chunk.offset
+    # thrust::pair<size_t, Envelope<Point<double,2>>>: 8-byte id then 32 bytes
+    assert sizes[9] == 40 == ctypes.sizeof(L.rts_update_entry_f64) and sizes[10] == 8
+    assert sizes[11] == L.rts_config.coord_bits.offset
 
 
 def test_config_defaults_follow_reference():

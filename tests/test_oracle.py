@@ -136,3 +136,85 @@ def test_grid_filter_is_sound(oracle, kind):
     t0, c0, p0 = oracle.run(kind, boxes, qs, grid=False)
     t1, c1, p1 = oracle.run(kind, boxes, qs, grid=True)
     assert t0 == t1 and np.array_equal(c0, c1) and np.array_equal(p0, p1)
+
+
+# ---- double indexes (SpatialIndex<double, 2>) --------------------------------
+def _adversarial_pairs64(rng, n):
+    """Double pairs around the places the double predicates are decided:
+    coordinates a few double ulps apart, halfway between two floats (the
+    contains predicates compare float-rounded values), zero extents,
+    inversions, deleted boxes (max = min) and large magnitudes."""
+    a = rng.random((n, 4))
+    a[:, 2:] = a[:, :2] + rng.random((n, 2)) * 0.1
+    b = a.copy()
+    for c in range(4):
+        k = rng.integers(-3, 4, n)
+        step = np.where(k > 0, np.inf, -np.inf)
+        for _ in range(3):
+            sel = rng.random(n) < 0.5
+            b[sel, c] = np.nextafter(b[sel, c], step[sel])
+    # halfway between neighbouring floats: rounding to float decides contains
+    for arr in (a, b):
+        sel = rng.random(n) < 0.3
+        f = arr[sel].astype(np.float32)
+        up = np.nextafter(f, np.float32(np.inf))
+        mid = (f.astype(np.float64) + up.astype(np.float64)) / 2
+        jitter = rng.integers(-1, 2, mid.shape)
+        arr[sel] = np.where(jitter < 0, np.nextafter(mid, -np.inf),
+                            np.where(jitter > 0, np.nextafter(mid, np.inf), mid))
+    sel = rng.random(n) < 0.15
+    b[sel, 2] = b[sel, 0]
+    sel = rng.random(n) < 0.15
+    b[sel, 3] = b[sel, 1]
+    sel = rng.random(n) < 0.1
+    b[sel] = b[sel][:, [2, 1, 0, 3]]
+    sel = rng.random(n) < 0.1
+    a[sel, 2:] = a[sel, :2]     # deleted geometry
+    scale = np.where(rng.random(n) < 0.2, 1e5, 1.0)
+    return a * scale[:, None], b * scale[:, None]
+
+
+def test_double_slab_constant(oracle):
+    assert oracle.slab_k64() == 1.0 + 6.0 * 2.0 ** -52
+
+
+def test_double_port_matches_reference_predicates(oracle, ref_oracle):
+    rng = np.random.default_rng(21)
+    g, q = _adversarial_pairs64(rng, 200000)
+    for kind in (KIND_CONTAINS, KIND_INTERSECTS):
+        assert np.array_equal(oracle.eval_pairs64(kind, g, q), ref_oracle.eval_pairs64(kind, g, q))
+        assert np.array_equal(oracle.eval_pairs64(kind, q, g), ref_oracle.eval_pairs64(kind, q, g))
+    pts = np.concatenate([q[:, :2], q[:, 2:]])
+    gg = np.concatenate([g, g])
+    assert np.array_equal(oracle.eval_pairs64(KIND_POINT, gg, pts),
+                          ref_oracle.eval_pairs64(KIND_POINT, gg, pts))
+
+
+def test_double_contains_compares_float_rounded_coordinates(oracle):
+    # A point between a box's double max and the next float above it is
+    # contained: both round to the same float (geom/point.cuh:68-71).
+    f = np.float32(0.5)
+    up = float(np.nextafter(f, np.float32(1)))
+    box = np.array([[0.25, 0.25, float(f) + 1e-12, 0.75]])
+    inside_as_float = np.array([[float(f) + (up - float(f)) * 0.25, 0.5]])
+    assert oracle.eval_pairs64(KIND_POINT, box, inside_as_float)[0] == 1
+    outside = np.array([[up, 0.5]])
+    assert oracle.eval_pairs64(KIND_POINT, box, outside)[0] == 0
+    # ... while validity (used by intersects) compares the doubles
+    thin = np.array([[0.5, 0.5, 0.5 + 1e-12, 0.6]])   # float-rounded: zero width
+    q = np.array([[0.4, 0.55, 0.6, 0.56]])
+    assert oracle.eval_pairs64(KIND_INTERSECTS, thin, q)[0] == 1
+
+
+def test_double_bulk_matches_pairwise(oracle, ref_oracle):
+    rng = np.random.default_rng(22)
+    g, q = _adversarial_pairs64(rng, 3000)
+    for kind, qs in ((KIND_POINT, q[:400, :2]), (KIND_CONTAINS, q[:400]), (KIND_INTERSECTS, q[:400])):
+        total, counts, pairs = oracle.run64(kind, g, qs)
+        want = []
+        for j in range(qs.shape[0]):
+            hits = np.nonzero(oracle.eval_pairs64(kind, g, np.repeat(qs[j:j + 1], g.shape[0], 0)))[0]
+            want.extend((int(h), j) for h in hits)
+        assert total == len(want)
+        assert pairs.tolist() == [list(p) for p in want]
+        assert ref_oracle.run64(kind, g, qs)[0] == total
