@@ -511,7 +511,9 @@ def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1)
     the order-key kernel and the radix sort's histogram, scan and one
     onesweep pass per 8 key bits when queries are curve-sorted, plus the
     query gather of a merged launch (several batches of one predicate that
-    count or use the packet scheme, sorted together on 32-bit keys)."""
+    count or use the packet scheme, sorted together on 32-bit keys), or, for
+    an unmerged launch of several batches, the chunk-order key kernel and its
+    32-bit sort (histogram, scan, 4 passes)."""
     sorted_ = cfg.sort_queries == 1 or (cfg.sort_queries == 2 and nq >= 8192)
     if not sorted_:
         return 1
@@ -520,7 +522,8 @@ def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1)
     end_bit = 32
     while not merged and end_bit < 64 and (1 << (end_bit - 32)) < nbatch:
         end_bit += 1
-    return 1 + 1 + 2 + (end_bit + 7) // 8 + (1 if merged else 0)
+    chunk_order = nbatch > 1 and not merged and cfg.traversal != 3
+    return 1 + 1 + 2 + (end_bit + 7) // 8 + (1 if merged else 0) + (7 if chunk_order else 0)
 
 
 def run_mutable_bench(args, ctx):

@@ -119,9 +119,9 @@ typedef struct rts_config {
   float rebuild_update_fraction; /* updates since the last rebuild, as a fraction of the index,
                                     above which Update re-sorts instead of refitting */
   uint32_t chunk;         /* queries per device work item (0 = library default) */
-  int32_t query_occupancy; /* 2 / 4: query kernel capped at 128 / 64 registers (2 / 4 CTAs
-                              of 256 threads per SM); 1: uncapped; 0: per scheme (thread 2,
-                              packet 4, team 1) */
+  int32_t query_occupancy; /* 2 / 3 / 4: query kernel capped at 128 / 80 / 64 registers
+                              (2 / 3 / 4 CTAs of 256 threads per SM); 1: uncapped; 0: per
+                              scheme (thread 2, packet 4, team 1) */
   float frontier_factor;   /* frontier traversal: entries per query of each level buffer
                               (queries beyond it are answered depth-first); 0 = 16 */
   int32_t coord_bits;      /* 32: SpatialIndex<float, 2>; 64: SpatialIndex<double, 2>, whose
@@ -165,7 +165,11 @@ int rts_delete(rts_index* index, const uint64_t* ids, uint64_t n, void* stream);
 
 /* SpatialIndex::Update (spatial_index.cuh:280-336): overwrites the listed
  * envelopes.  Every id must be < size (the reference asserts it, :295);
- * out-of-range entries are skipped here. */
+ * out-of-range entries are skipped here; an id listed twice keeps one of its
+ * envelopes.  An envelope that stays inside its leaf group's hull is written
+ * in place; one that leaves it moves, with its id, to a new sub-tree (the
+ * reference refits instead, letting every hull above it grow).  Waits for the
+ * stream once (to size that sub-tree). */
 int rts_update(rts_index* index, const rts_update_entry* updates, uint64_t n, void* stream);
 
 /* SpatialIndex::Query(Predicate, ArrayView<point_t>, void*, cudaStream_t)

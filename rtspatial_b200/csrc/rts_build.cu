@@ -150,16 +150,6 @@ __global__ void k_pack(const float4* __restrict__ in, uint64_t n_in, float4* __r
   if ((i & ((1u << log2g) - 1)) == 0 && j < n_out_pad) out[j] = b;
 }
 
-__global__ void k_slot_list(const uint64_t* __restrict__ meta, int n_trees,
-                            uint32_t* __restrict__ slots) {
-  // meta: per tree {id_begin, n, slot_base}
-  int t = blockIdx.y;
-  if (t >= n_trees) return;
-  uint64_t id_begin = meta[3 * t], n = meta[3 * t + 1], slot_base = meta[3 * t + 2];
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    slots[id_begin + i] = static_cast<uint32_t>(slot_base + i);
-}
 
 // Delete: Envelope::Invalid() (max := min) on each listed id below n_ids
 // (spatial_index.cuh:216-233); the box stays in its slot.
@@ -178,28 +168,83 @@ __global__ void k_delete(const uint64_t* __restrict__ ids, uint64_t n, uint64_t 
   if (leaves64) leaves64[slot].hi = leaves64[slot].lo;  // Invalid(): max := min in double
 }
 
-// Update: overwrite the envelope of each listed id (spatial_index.cuh:289-305).
-__global__ void k_update(const rts_update_entry* __restrict__ upd, uint64_t n, uint64_t n_ids,
-                         const uint32_t* __restrict__ pos, float4* __restrict__ leaves) {
-  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  rts_update_entry e = upd[i];
-  if (e.id >= n_ids) return;
-  leaves[pos[e.id]] = make_float4(e.min_x, e.min_y, e.max_x, e.max_y);
+
+
+// ---- Update split ------------------------------------------------------------
+// An updated envelope that stays inside the hull of its leaf group (the
+// level-1 entry above its slot) is written in place: no hull has to grow.  One
+// that leaves it would stretch every hull up to the root, so its slot becomes
+// an empty box (matches nothing) and the envelope moves, with its id, to a new
+// sub-tree (rts_update builds it like an insert).  Decided per slot: pass 1
+// marks the slots with an outward update, pass 2 writes the unmarked slots in
+// place and lets one update per marked slot claim the move, so an id listed
+// twice still ends up with exactly one envelope.
+
+__device__ __forceinline__ bool slot_keeps(const UpdateTrees& T, uint32_t slot, float4 b) {
+  for (uint32_t t = 0; t < T.n_trees; ++t) {
+    if (slot >= T.slot_base[t] && slot < T.slot_end[t]) {
+      const float4 H = T.group_hull[t][(slot - T.slot_base[t]) >> T.log2w];
+      const float4 h = hull(b);
+      return H.x <= h.x && H.y <= h.y && h.z <= H.z && h.w <= H.w;
+    }
+  }
+  return false;
 }
 
-// Double index: the double envelope and its float rounding.
-__global__ void k_update64(const rts_update_entry_f64* __restrict__ upd, uint64_t n,
-                           uint64_t n_ids, const uint32_t* __restrict__ pos,
-                           float4* __restrict__ leaves, DBox* __restrict__ leaves64) {
+__device__ __forceinline__ void set_bit(uint32_t* bits, uint32_t i) {
+  atomicOr(bits + (i >> 5), 1u << (i & 31));
+}
+
+template <typename E>
+__device__ __forceinline__ float4 entry_box(const E& e) {
+  if constexpr (sizeof(e.min_x) == 8)
+    return round_box(DBox{make_double2(e.min_x, e.min_y), make_double2(e.max_x, e.max_y)});
+  else
+    return make_float4(e.min_x, e.min_y, e.max_x, e.max_y);
+}
+
+template <typename E>
+__global__ void k_update_mark(const E* __restrict__ upd, uint64_t n, uint64_t n_ids,
+                              const uint32_t* __restrict__ pos, const UpdateTrees T,
+                              uint32_t* __restrict__ moves) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  rts_update_entry_f64 e = upd[i];
+  const E e = upd[i];
   if (e.id >= n_ids) return;
-  const DBox b{make_double2(e.min_x, e.min_y), make_double2(e.max_x, e.max_y)};
   const uint32_t slot = pos[e.id];
-  leaves64[slot] = b;
-  leaves[slot] = round_box(b);
+  if (!slot_keeps(T, slot, entry_box(e))) set_bit(moves, slot);
+}
+
+template <typename E>
+__global__ void k_update_apply(const E* __restrict__ upd, uint64_t n, uint64_t n_ids,
+                               const uint32_t* __restrict__ pos, float4* __restrict__ leaves,
+                               DBox* __restrict__ leaves64, const uint32_t* __restrict__ moves,
+                               uint32_t* __restrict__ claimed, uint32_t* __restrict__ moved_ids,
+                               float4* __restrict__ moved, DBox* __restrict__ moved64,
+                               uint32_t* __restrict__ n_moved) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const E e = upd[i];
+  if (e.id >= n_ids) return;
+  const uint32_t slot = pos[e.id];
+  const float4 b = entry_box(e);
+  DBox b64{};
+  if constexpr (sizeof(e.min_x) == 8)
+    b64 = DBox{make_double2(e.min_x, e.min_y), make_double2(e.max_x, e.max_y)};
+  const uint32_t bit = 1u << (slot & 31);
+  if (!(moves[slot >> 5] & bit)) {  // stays: in place
+    leaves[slot] = b;
+    if (leaves64) leaves64[slot] = b64;
+    return;
+  }
+  if (atomicOr(claimed + (slot >> 5), bit) & bit) return;  // another update moves this id
+  leaves[slot] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
+  if (leaves64)
+    leaves64[slot] = DBox{make_double2(INFINITY, INFINITY), make_double2(-INFINITY, -INFINITY)};
+  const uint32_t k = atomicAdd(n_moved, 1u);
+  moved_ids[k] = static_cast<uint32_t>(e.id);
+  moved[k] = b;
+  if (moved64) moved64[k] = b64;
 }
 
 // Double index: float rounding of inserted envelopes.
@@ -398,17 +443,6 @@ int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_
   return RTS_OK;
 }
 
-int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint32_t* slots,
-                     cudaStream_t s) {
-  if (n_trees == 0) return RTS_OK;
-  uint64_t gx = div_up(max_n, kThreads);
-  if (gx > 4096) gx = 4096;
-  if (gx == 0) gx = 1;
-  dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(n_trees));
-  k_slot_list<<<grid, kThreads, 0, s>>>(meta_dev, n_trees, slots);
-  RTS_CUDA_TRY(cudaGetLastError());
-  return RTS_OK;
-}
 
 int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
                        const float4* frame_box, int curve, unsigned long long* keys_a,
@@ -484,21 +518,41 @@ int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_
   return RTS_OK;
 }
 
-int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
-                  float4* leaves, cudaStream_t s) {
+
+template <typename E>
+int launch_update_split_t(const E* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
+                          const UpdateTrees& T, uint64_t slot_end, float4* leaves, DBox* leaves64,
+                          uint32_t* bits, uint32_t* moved_ids, float4* moved, DBox* moved64,
+                          uint32_t* n_moved, cudaStream_t s) {
+  const uint64_t words = (slot_end + 31) / 32;
+  RTS_CUDA_TRY(cudaMemsetAsync(bits, 0, 2 * words * sizeof(uint32_t), s));
+  RTS_CUDA_TRY(cudaMemsetAsync(n_moved, 0, sizeof(uint32_t), s));
   if (n == 0) return RTS_OK;
-  k_update<<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, leaves);
+  k_update_mark<E><<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, T, bits);
+  RTS_CUDA_TRY(cudaGetLastError());
+  k_update_apply<E><<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, leaves, leaves64, bits,
+                                                     bits + words, moved_ids, moved, moved64,
+                                                     n_moved);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }
 
-int launch_update64(const rts_update_entry_f64* upd, uint64_t n, uint64_t n_ids,
-                    const uint32_t* pos, float4* leaves, DBox* leaves64, cudaStream_t s) {
-  if (n == 0) return RTS_OK;
-  k_update64<<<grid_for(n), kThreads, 0, s>>>(upd, n, n_ids, pos, leaves, leaves64);
-  RTS_CUDA_TRY(cudaGetLastError());
-  return RTS_OK;
+int launch_update_split(const rts_update_entry* upd, uint64_t n, uint64_t n_ids,
+                        const uint32_t* pos, const UpdateTrees& T, uint64_t slot_end,
+                        float4* leaves, uint32_t* bits, uint32_t* moved_ids, float4* moved,
+                        uint32_t* n_moved, cudaStream_t s) {
+  return launch_update_split_t(upd, n, n_ids, pos, T, slot_end, leaves, nullptr, bits, moved_ids,
+                               moved, nullptr, n_moved, s);
 }
+
+int launch_update_split64(const rts_update_entry_f64* upd, uint64_t n, uint64_t n_ids,
+                          const uint32_t* pos, const UpdateTrees& T, uint64_t slot_end,
+                          float4* leaves, DBox* leaves64, uint32_t* bits, uint32_t* moved_ids,
+                          float4* moved, DBox* moved64, uint32_t* n_moved, cudaStream_t s) {
+  return launch_update_split_t(upd, n, n_ids, pos, T, slot_end, leaves, leaves64, bits, moved_ids,
+                               moved, moved64, n_moved, s);
+}
+
 
 int launch_round_boxes(const DBox* in, uint64_t n, float4* out, cudaStream_t s) {
   if (n == 0) return RTS_OK;

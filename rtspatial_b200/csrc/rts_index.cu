@@ -177,22 +177,11 @@ int rebuild_all(rts_index* ix, cudaStream_t s) {
 int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
   const uint64_t N = ix->n_ids;
   int rc;
-  // slots_tmp[k] = slot of the k-th id-ordered entry, tree by tree.
-  std::vector<uint64_t> meta;
-  uint64_t max_n = 0;
-  for (auto& t : ix->trees) {
-    meta.push_back(t.id_begin);
-    meta.push_back(t.n);
-    meta.push_back(t.slot_base);
-    max_n = std::max(max_n, t.n);
-  }
-  void* meta_dev = nullptr;
-  if ((rc = ix->staging.put(meta.data(), meta.size() * sizeof(uint64_t), s, &meta_dev))) return rc;
+  // slots_tmp[id] = the current slot of each id (pos); slots emptied by
+  // moved updates are not listed and drop out.
   if ((rc = buf_reserve(ix->slots_tmp, N * sizeof(uint32_t), s, false, 0))) return rc;
   auto* slots = static_cast<uint32_t*>(ix->slots_tmp.ptr);
-  if ((rc = launch_slot_list(static_cast<const uint64_t*>(meta_dev), static_cast<int>(ix->trees.size()),
-                             max_n, slots, s)))
-    return rc;
+  RTS_CUDA_TRY(cudaMemcpyAsync(slots, pos_of(ix), N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   // New slot arrays; the old ones are read by the gather.
   DevBuf new_leaves, new_ids, new_leaves64;
   const uint64_t slots_needed = round_up(N, kSlotAlign);
@@ -242,8 +231,15 @@ int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
   return RTS_OK;
 }
 
-void refresh_forest(rts_index* ix) {
-  if (!ix->forest_dirty) return;
+int refresh_forest(rts_index* ix) {
+  if (!ix->forest_dirty) return RTS_OK;
+  // The thread scheme reads two boxes per 32-byte load (ldg_box_pair): every
+  // buffer the groups live in must start on a 32-byte boundary (device
+  // allocations start on 256-byte ones; this only guards that assumption).
+  const auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; };
+  bool ok = aligned(ix->leaves.ptr);
+  for (const auto& t : ix->trees) ok = ok && aligned(t.nodes.ptr);
+  if (!ok) return fail(RTS_ERR_CUDA, "index buffer not 32-byte aligned");
   Forest& F = ix->forest;
   std::memset(&F, 0, sizeof(F));
   F.n_trees = static_cast<uint32_t>(ix->trees.size());
@@ -264,6 +260,7 @@ void refresh_forest(rts_index* ix) {
     }
   }
   ix->forest_dirty = false;
+  return RTS_OK;
 }
 
 LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
@@ -289,7 +286,7 @@ LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   p.chunk = static_cast<uint32_t>(std::max<uint64_t>(32, std::min<uint64_t>(chunk, fair)));
   int occ = ix->cfg.query_occupancy;
   if (occ == 0) occ = p.packet ? 4 : (p.team ? 1 : 2);  // library default per scheme
-  p.min_blocks = occ >= 4 ? 4 : (occ >= 2 ? 2 : 1);
+  p.min_blocks = occ >= 4 ? 4 : (occ == 3 ? 3 : (occ == 2 ? 2 : 1));
   return p;
 }
 
@@ -510,7 +507,7 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   if (n == 0 || ix->n_ids == 0) return RTS_OK;  // spatial_index.cuh:354-356
   if (!q) return fail(RTS_ERR_INVALID_ARGUMENT, "queries is null");
   if (n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in one call");
-  refresh_forest(ix);
+  if ((rc = refresh_forest(ix))) return rc;
   if ((rc = buf_reserve(ix->qs.work, sizeof(uint32_t), s, false, 0))) return rc;
   BatchDesc b{};
   b.queries = q;
@@ -608,7 +605,8 @@ int rts_destroy(rts_index* ix) {
   }
   DevBuf* all[] = {&ix->leaves, &ix->leaf_ids, &ix->pos, &ix->keys_a, &ix->keys_b, &ix->vals_a,
                    &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp, &ix->leaves64,
-                   &ix->rounded};
+                   &ix->rounded, &ix->upd_bits, &ix->upd_ids, &ix->upd_boxes,
+                   &ix->upd_boxes64, &ix->upd_count};
   for (DevBuf* b : all) {
     touched |= b->ptr != nullptr;
     buf_free(*b, s);
@@ -640,27 +638,30 @@ int rts_clear(rts_index* ix, void* stream) {
 
 namespace rts {
 
-// Insert of n envelopes given as floats (src) and, for a double index, as
-// doubles (src64; src is then their float rounding).
-int insert_impl(rts_index* ix, const float4* src, const DBox* src64, uint64_t n, cudaStream_t s) {
-  if (ix->n_ids + n >= 0xffffffffull)
+// A new sub-tree of n envelopes given as floats (src) and, for a double
+// index, as doubles (src64; src is then their float rounding).  ids == nullptr:
+// an Insert (new ids n_ids, n_ids + 1, ...); else the envelopes keep the
+// listed ids (updates moved out of their leaf group).
+int insert_impl(rts_index* ix, const float4* src, const DBox* src64, const uint32_t* ids,
+                uint64_t n, cudaStream_t s) {
+  if (!ids && ix->n_ids + n >= 0xffffffffull)
     return fail(RTS_ERR_CAPACITY, "ids are 32-bit: at most 2^32-2 envelopes per index");
   int rc;
   const uint64_t slot_base = ix->slot_end;
   const uint64_t slot_end = slot_base + round_up(n, kSlotAlign);
   if ((rc = ensure_slots(ix, slot_end, s))) return rc;
-  if ((rc = ensure_ids(ix, ix->n_ids + n, s))) return rc;
-  if ((rc = sort_into_slots(ix, src, nullptr, nullptr, n, ix->n_ids, slot_base, leaves_of(ix),
-                            ids_of(ix), s, src64, leaves64_of(ix))))
+  if (!ids && (rc = ensure_ids(ix, ix->n_ids + n, s))) return rc;
+  if ((rc = sort_into_slots(ix, src, ids, nullptr, n, ids ? 0 : ix->n_ids, slot_base,
+                            leaves_of(ix), ids_of(ix), s, src64, leaves64_of(ix))))
     return rc;
   HostTree t;
-  t.id_begin = ix->n_ids;
+  t.id_begin = ids ? 0 : ix->n_ids;
   t.n = n;
   t.slot_base = slot_base;
   const bool merge = !ix->trees.empty() &&
                      (static_cast<int>(ix->trees.size()) >= ix->cfg.max_trees ||
                       static_cast<double>(n) > ix->cfg.rebuild_fraction * static_cast<double>(ix->n_ids));
-  ix->n_ids += n;
+  if (!ids) ix->n_ids += n;
   ix->slot_end = slot_end;
   ix->forest_dirty = true;
   ix->version++;
@@ -673,16 +674,53 @@ int insert_impl(rts_index* ix, const float4* src, const DBox* src64, uint64_t n,
   return RTS_OK;
 }
 
-// After n envelopes were overwritten: refit every sub-tree, or re-sort once
-// the updates since the last build pass the configured fraction.
-int after_update(rts_index* ix, uint64_t n, cudaStream_t s) {
+// Update of n entries (rts_update_entry, or rts_update_entry_f64 for a double
+// index): envelopes that stay inside their leaf group's hull are written in
+// place (no hull grows, so nothing is refit); the others leave an empty slot
+// and move, with their ids, to a new sub-tree.  Re-sorts everything once the
+// updates since the last build pass rebuild_update_fraction of the index.
+int update_impl(rts_index* ix, const void* upd, uint64_t n, cudaStream_t s) {
+  int rc;
+  UpdateTrees T{};
+  T.n_trees = static_cast<uint32_t>(ix->trees.size());
+  while ((1u << T.log2w) < static_cast<uint32_t>(ix->W)) ++T.log2w;
+  for (size_t i = 0; i < ix->trees.size(); ++i) {
+    const HostTree& h = ix->trees[i];
+    T.slot_base[i] = h.slot_base;
+    T.slot_end[i] = h.slot_base + round_up(h.n, kSlotAlign);
+    T.group_hull[i] = static_cast<const float4*>(h.nodes.ptr) + h.level_off[1];
+  }
+  const uint64_t words = (ix->slot_end + 31) / 32;
+  const bool f64 = is_f64(ix);
+  if ((rc = buf_reserve(ix->upd_bits, 2 * words * sizeof(uint32_t), s, false, 0)) ||
+      (rc = buf_reserve(ix->upd_ids, std::max<uint64_t>(n, 1) * sizeof(uint32_t), s, false, 0)) ||
+      (rc = buf_reserve(ix->upd_boxes, std::max<uint64_t>(n, 1) * sizeof(float4), s, false, 0)) ||
+      (rc = buf_reserve(ix->upd_count, sizeof(uint32_t), s, false, 0)) ||
+      (f64 && (rc = buf_reserve(ix->upd_boxes64, std::max<uint64_t>(n, 1) * sizeof(DBox), s,
+                                false, 0))))
+    return rc;
+  auto* bits = static_cast<uint32_t*>(ix->upd_bits.ptr);
+  auto* mids = static_cast<uint32_t*>(ix->upd_ids.ptr);
+  auto* mboxes = static_cast<float4*>(ix->upd_boxes.ptr);
+  auto* mboxes64 = f64 ? static_cast<DBox*>(ix->upd_boxes64.ptr) : nullptr;
+  auto* count = static_cast<uint32_t*>(ix->upd_count.ptr);
+  if (f64)
+    rc = launch_update_split64(static_cast<const rts_update_entry_f64*>(upd), n, ix->n_ids,
+                               pos_of(ix), T, ix->slot_end, leaves_of(ix), leaves64_of(ix), bits,
+                               mids, mboxes, mboxes64, count, s);
+  else
+    rc = launch_update_split(static_cast<const rts_update_entry*>(upd), n, ix->n_ids, pos_of(ix),
+                             T, ix->slot_end, leaves_of(ix), bits, mids, mboxes, count, s);
+  if (rc) return rc;
+  uint32_t moved = 0;
+  RTS_CUDA_TRY(cudaMemcpyAsync(&moved, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  RTS_CUDA_TRY(cudaStreamSynchronize(s));
   ix->updated_since_build += n;
+  // (a merge rebuild inside insert_impl resets updated_since_build)
+  if (moved && (rc = insert_impl(ix, mboxes, mboxes64, mids, moved, s))) return rc;
   if (static_cast<double>(ix->updated_since_build) >
       ix->cfg.rebuild_update_fraction * static_cast<double>(ix->n_ids))
     return rebuild_all(ix, s);
-  int rc;
-  for (auto& t : ix->trees)
-    if ((rc = launch_pack_tree(leaves_of(ix) + t.slot_base, t, ix->W, s))) return rc;
   return RTS_OK;
 }
 
@@ -702,7 +740,7 @@ int rts_insert(rts_index* ix, const float* envelopes, uint64_t n, void* stream) 
   if (rc) return rc;
   if (n == 0) return RTS_OK;  // spatial_index.cuh:144-146
   if (!envelopes) return fail(RTS_ERR_INVALID_ARGUMENT, "envelopes is null");
-  return insert_impl(ix, reinterpret_cast<const float4*>(envelopes), nullptr, n,
+  return insert_impl(ix, reinterpret_cast<const float4*>(envelopes), nullptr, nullptr, n,
                      static_cast<cudaStream_t>(stream));
 }
 
@@ -717,7 +755,7 @@ int rts_insert_f64(rts_index* ix, const double* envelopes, uint64_t n, void* str
   if ((rc = buf_reserve(ix->rounded, n * sizeof(float4), s, false, 0))) return rc;
   auto* rounded = static_cast<float4*>(ix->rounded.ptr);
   if ((rc = launch_round_boxes(src64, n, rounded, s))) return rc;
-  return insert_impl(ix, rounded, src64, n, s);
+  return insert_impl(ix, rounded, src64, nullptr, n, s);
 }
 
 int rts_delete(rts_index* ix, const uint64_t* ids, uint64_t n, void* stream) {
@@ -734,9 +772,7 @@ int rts_update(rts_index* ix, const rts_update_entry* upd, uint64_t n, void* str
   if (rc) return rc;
   if (n == 0 || ix->n_ids == 0) return RTS_OK;
   if (!upd) return fail(RTS_ERR_INVALID_ARGUMENT, "updates is null");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if ((rc = launch_update(upd, n, ix->n_ids, pos_of(ix), leaves_of(ix), s))) return rc;
-  return after_update(ix, n, s);
+  return update_impl(ix, upd, n, static_cast<cudaStream_t>(stream));
 }
 
 int rts_update_f64(rts_index* ix, const rts_update_entry_f64* upd, uint64_t n, void* stream) {
@@ -745,10 +781,7 @@ int rts_update_f64(rts_index* ix, const rts_update_entry_f64* upd, uint64_t n, v
   if (rc) return rc;
   if (n == 0 || ix->n_ids == 0) return RTS_OK;
   if (!upd) return fail(RTS_ERR_INVALID_ARGUMENT, "updates is null");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if ((rc = launch_update64(upd, n, ix->n_ids, pos_of(ix), leaves_of(ix), leaves64_of(ix), s)))
-    return rc;
-  return after_update(ix, n, s);
+  return update_impl(ix, upd, n, static_cast<cudaStream_t>(stream));
 }
 
 int rts_query_points(rts_index* ix, int predicate, const float* points, uint64_t n, int handler,
@@ -804,7 +837,7 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   int rc = make_descs(ix, batches, n_batches, plan, descs, chunks);
   if (rc) return rc;
   if (descs.empty() || ix->n_ids == 0) return RTS_OK;
-  refresh_forest(ix);
+  if ((rc = refresh_forest(ix))) return rc;
   if ((rc = buf_reserve(ix->qs.work, sizeof(uint32_t), s, false, 0))) return rc;
   uint64_t total = 0;
   for (const auto& d : descs) total += d.n;
@@ -978,7 +1011,7 @@ extern "C" int rts_query_batched_noalloc(rts_index* ix, const rts_batch* batches
   if (nd == 0 || ix->n_ids == 0) return RTS_OK;
   void* scratch = nullptr;
   if ((rc = noalloc_scratch(&scratch))) return rc;
-  refresh_forest(ix);
+  if ((rc = refresh_forest(ix))) return rc;
   auto* counter = static_cast<uint32_t*>(scratch);
   auto* ddescs = reinterpret_cast<BatchDesc*>(static_cast<unsigned char*>(scratch) +
                                               kNoAllocCounterBytes);

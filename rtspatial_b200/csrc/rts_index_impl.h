@@ -93,6 +93,8 @@ struct rts_index {
   rts::DevBuf leaves, leaf_ids, pos;
   rts::DevBuf leaves64;         // double index: the double envelopes, slot by slot
   rts::DevBuf rounded;          // double index: scratch of an insert's float rounding
+  // scratch of the update split: slot bitmaps, moved ids / envelopes, count
+  rts::DevBuf upd_bits, upd_ids, upd_boxes, upd_boxes64, upd_count;
   std::vector<rts::HostTree> trees;
   // scratch of the build path
   rts::DevBuf keys_a, keys_b, vals_a, vals_b, sort_temp, bounds, slots_tmp;
@@ -120,7 +122,7 @@ inline DBox* leaves64_of(rts_index* ix) {
   return is_f64(ix) ? static_cast<DBox*>(ix->leaves64.ptr) : nullptr;
 }
 
-void refresh_forest(rts_index* ix);
+int refresh_forest(rts_index* ix);
 // Re-sorts every box of the index into one tree at the index's node width.
 int rebuild_all(rts_index* ix, cudaStream_t s);
 LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total_queries);

@@ -67,12 +67,8 @@ int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* or
 // Empty boxes (+inf, +inf, -inf, -inf) in slots [from, to); ids = ~0.
 int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s,
                     DBox* leaves64 = nullptr);
-// Levels 1..top and the root box of a tree from its leaves (also the refit).
+// Levels 1..top and the root box of a tree from its leaves.
 int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_t s);
-// slots[id_begin_t + i] = slot_base_t + i for every tree t; meta (device) =
-// {id_begin, n, slot_base} per tree.
-int launch_slot_list(const uint64_t* meta_dev, int n_trees, uint64_t max_n, uint32_t* slots,
-                     cudaStream_t s);
 // Visiting order of the queries of nb batches: sorts (batch, curve key of the
 // query centre) and writes each batch's query indices to order[qbase ...].
 // With `merged` (every batch of one predicate, nb > 1) the queries of all
@@ -97,10 +93,26 @@ int chunk_order_temp_bytes(uint32_t total_chunks, size_t* bytes);
 int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes);
 int launch_delete(const uint64_t* ids, uint64_t n, uint64_t n_ids, const uint32_t* pos,
                   float4* leaves, cudaStream_t s, DBox* leaves64 = nullptr);
-int launch_update(const rts_update_entry* upd, uint64_t n, uint64_t n_ids, const uint32_t* pos,
-                  float4* leaves, cudaStream_t s);
-int launch_update64(const rts_update_entry_f64* upd, uint64_t n, uint64_t n_ids,
-                    const uint32_t* pos, float4* leaves, DBox* leaves64, cudaStream_t s);
+
+// Slot ranges and leaf-group hulls of the sub-trees, for the update split.
+struct UpdateTrees {
+  uint64_t slot_base[kMaxTrees];
+  uint64_t slot_end[kMaxTrees];
+  const float4* group_hull[kMaxTrees];  // level-1 entries: hull of each W-group of leaves
+  uint32_t n_trees;
+  uint32_t log2w;
+};
+// Update with envelopes that leave their leaf group's hull moved out (their
+// slot emptied, (id, envelope) appended to moved / moved64, *n_moved counted);
+// the rest written in place.  bits: 2 * ceil(slot_end / 32) words of scratch.
+int launch_update_split(const rts_update_entry* upd, uint64_t n, uint64_t n_ids,
+                        const uint32_t* pos, const UpdateTrees& T, uint64_t slot_end,
+                        float4* leaves, uint32_t* bits, uint32_t* moved_ids, float4* moved,
+                        uint32_t* n_moved, cudaStream_t s);
+int launch_update_split64(const rts_update_entry_f64* upd, uint64_t n, uint64_t n_ids,
+                          const uint32_t* pos, const UpdateTrees& T, uint64_t slot_end,
+                          float4* leaves, DBox* leaves64, uint32_t* bits, uint32_t* moved_ids,
+                          float4* moved, DBox* moved64, uint32_t* n_moved, cudaStream_t s);
 // out[i] = the double envelope in[i] rounded to nearest float.
 int launch_round_boxes(const DBox* in, uint64_t n, float4* out, cudaStream_t s);
 
@@ -133,7 +145,7 @@ struct LaunchPlan {
   bool frontier = false;      // breadth-first pass (plus depth-first fallback)
   bool packet = false;        // warp-per-packet depth-first scheme
   uint32_t chunk = 32;  // queries per work item
-  int min_blocks = 1;         // CTAs of 256 threads per SM the registers are capped for (1, 2, 4)
+  int min_blocks = 1;         // CTAs of 256 threads per SM the registers are capped for (1-4)
   bool merged = false;        // sort the queries of all batches together (MergedOrder)
   bool chunk_order = false;   // sorted, unmerged, several batches: chunks visited by space
 };

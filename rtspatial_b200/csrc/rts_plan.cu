@@ -37,10 +37,10 @@ void drop_graph(rts_plan* p) {
 // The launch sequence: [order keys + sort], work-counter reset, query kernel.
 int enqueue(rts_plan* p, cudaStream_t s) {
   rts_index* ix = p->ix;
-  refresh_forest(ix);
+  int rc = refresh_forest(ix);
+  if (rc) return rc;
   const uint32_t nd = static_cast<uint32_t>(p->descs.size());
   const BatchDesc* dd = static_cast<const BatchDesc*>(p->ddescs.ptr);
-  int rc;
   if (p->sorted && (rc = fill_order(ix, p->qs, p->plan, p->descs.data(), nd > 1 ? dd : nullptr, nd,
                                     p->total, p->chunks, s)))
     return rc;
@@ -109,7 +109,7 @@ int rts_plan_launch(rts_plan* p, void* stream, int use_graph) {
     drop_graph(p);
     if (!p->capture_stream)
       RTS_CUDA_TRY(cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking));
-    refresh_forest(p->ix);
+    if (int rc = refresh_forest(p->ix)) return rc;
     RTS_CUDA_TRY(cudaStreamBeginCapture(p->capture_stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue(p, p->capture_stream);
     cudaGraph_t g = nullptr;

@@ -215,6 +215,7 @@ static QueryKernel pick_kernel_occ(const LaunchPlan& p) {
 static QueryKernel pick_kernel(const LaunchPlan& p, bool routed) {
   switch (p.min_blocks) {
     case 4: return routed ? pick_kernel_occ<4, true>(p) : pick_kernel_occ<4, false>(p);
+    case 3: return routed ? pick_kernel_occ<3, true>(p) : pick_kernel_occ<3, false>(p);
     case 2: return routed ? pick_kernel_occ<2, true>(p) : pick_kernel_occ<2, false>(p);
     default: return routed ? pick_kernel_occ<1, true>(p) : pick_kernel_occ<1, false>(p);
   }

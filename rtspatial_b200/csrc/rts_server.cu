@@ -364,7 +364,7 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
     e = cudaMemcpyAsync(sl.d_descs.ptr, sl.h_descs, np * sizeof(BatchDesc), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_counts, 0, np * sizeof(uint32_t), s);
   if (e != cudaSuccess) rc = cuda_fail(e, "server launch staging");
-  refresh_forest(ix);
+  if (!rc) rc = refresh_forest(ix);
   const BatchDesc* dd = static_cast<const BatchDesc*>(sl.d_descs.ptr);
   if (!rc && sorted)
     rc = fill_order(ix, sl.qs, plan, sl.h_descs, np > 1 ? dd : nullptr, np, total, chunks, s);

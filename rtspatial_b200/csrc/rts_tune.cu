@@ -137,10 +137,12 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
       {RTS_TRAVERSAL_THREAD, 2, 1, 64},   {RTS_TRAVERSAL_THREAD, 2, 0, 64},
       {RTS_TRAVERSAL_THREAD, 2, 1, 128},  {RTS_TRAVERSAL_THREAD, 2, 0, 128},
       {RTS_TRAVERSAL_THREAD, 4, 1, 64},   {RTS_TRAVERSAL_THREAD, 4, 1, 128},
+      {RTS_TRAVERSAL_THREAD, 3, 1, 64},   {RTS_TRAVERSAL_THREAD, 3, 1, 128},
       {RTS_TRAVERSAL_TEAM, 1, 1, 64},     {RTS_TRAVERSAL_TEAM, 4, 1, 128},
       {RTS_TRAVERSAL_FRONTIER, 4, 0, 64}, {RTS_TRAVERSAL_FRONTIER, 4, 1, 64},
       {RTS_TRAVERSAL_PACKET, 1, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 64},
       {RTS_TRAVERSAL_PACKET, 2, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 256},
+      {RTS_TRAVERSAL_PACKET, 3, 1, 64},
   };
   double best = 1e300, first = -1;
   int best_w = ix->W;

@@ -1,6 +1,7 @@
 """Insert / Delete / Update sequences against the oracle: after every step the
 GPU's pair sets equal the oracle's over the same (mutated) box array.  Covers
-sub-tree inserts, merge rebuilds, refits and update-triggered re-sorts."""
+sub-tree inserts, merge rebuilds, in-place updates, updates moved to a new
+sub-tree, ids updated twice in one call and update-triggered re-sorts."""
 import numpy as np
 import pytest
 import torch
@@ -86,3 +87,59 @@ def test_deleted_box_semantics(cuda, oracle):
                       "intersects")
     assert_same_pairs(gpu_pairs(ix, P.kContains, qs), oracle.run(KIND_CONTAINS, b, qs)[2],
                       "contains")
+
+
+@pytest.mark.parametrize("w,t", [(16, rb._lib.RTS_TRAVERSAL_THREAD), (32, rb._lib.RTS_TRAVERSAL_PACKET),
+                                 (8, rb._lib.RTS_TRAVERSAL_TEAM)], ids=["w16-thread", "w32-packet",
+                                                                        "w8-team"])
+def test_update_moves_far_envelopes_to_a_new_subtree(cuda, oracle, w, t):
+    # Updates to random far positions leave their leaf group: their slots are
+    # emptied and they move (same ids) into a new sub-tree; small moves stay.
+    rng = np.random.default_rng(5 + w)
+    boxes = wl.uniform_boxes(rng, 40_000, 5e-3)
+    pts = wl.uniform_points(rng, 3000)
+    qs = wl.uniform_boxes(rng, 3000, 2e-2)
+    ix = rb.SpatialIndex(rb.Config(node_width=w, traversal=t, max_trees=8,
+                                   rebuild_update_fraction=0.9))
+    ix.Insert(dev(boxes))
+    far = rng.choice(boxes.shape[0], 3000, replace=False)
+    near = np.setdiff1d(rng.choice(boxes.shape[0], 3000, replace=False), far)
+    ups = np.concatenate([far, near])
+    nb = np.concatenate([wl.uniform_boxes(rng, far.shape[0], 5e-3),
+                         boxes[near] + np.float32(1e-7)])
+    ix.Update(torch.from_numpy(ups.astype(np.int64)).cuda(), dev(nb))
+    cur = boxes.copy()
+    cur[ups] = nb
+    assert ix.num_trees() == 2     # the moved envelopes form one new sub-tree
+    check_all(ix, oracle, cur, pts, qs, "after far updates")
+    # deletes reach moved ids through their new slots
+    dels = far[:500]
+    ix.Delete(torch.from_numpy(dels.astype(np.int64)).cuda())
+    oracle.invalidate(cur, dels)
+    check_all(ix, oracle, cur, pts, qs, "after deleting moved ids")
+    # a re-sort keeps every id once (emptied slots drop out)
+    ix2 = rb.SpatialIndex(rb.Config(node_width=w, traversal=t, rebuild_update_fraction=0.0))
+    ix2.Insert(dev(boxes))
+    ix2.Update(torch.from_numpy(ups.astype(np.int64)).cuda(), dev(nb))
+    assert ix2.num_trees() == 1
+    cur2 = boxes.copy()
+    cur2[ups] = nb
+    check_all(ix2, oracle, cur2, pts, qs, "after re-sort")
+
+
+def test_update_listing_an_id_twice_keeps_one_envelope(cuda, oracle):
+    rng = np.random.default_rng(17)
+    boxes = wl.uniform_boxes(rng, 20_000, 5e-3)
+    qs = wl.uniform_boxes(rng, 4000, 5e-2)
+    ix = rb.SpatialIndex(rb.Config(rebuild_update_fraction=0.9))
+    ix.Insert(dev(boxes))
+    a = np.array([[0.1, 0.1, 0.3, 0.3]], np.float32)
+    b = np.array([[0.6, 0.6, 0.9, 0.9]], np.float32)
+    ix.Update(torch.tensor([7, 7], dtype=torch.int64).cuda(), dev(np.concatenate([a, b])))
+    got = gpu_pairs(ix, P.kIntersects, qs)
+    wants = []
+    for v in (a, b):
+        cur = boxes.copy()
+        cur[7] = v[0]
+        wants.append(oracle.run(KIND_INTERSECTS, cur, qs)[2])
+    assert any(got.shape == w_.shape and np.array_equal(got, w_) for w_ in wants)

@@ -134,7 +134,7 @@ def test_queue_overflow_reports_needed_size(cuda, oracle):
 
 @pytest.mark.parametrize("combo", SOME_COMBOS, ids=combo_id)
 @pytest.mark.parametrize("order", [0, 1], ids=["as-given", "curve-sorted"])
-@pytest.mark.parametrize("occ", [0, 4], ids=["occ-default", "occ-4"])
+@pytest.mark.parametrize("occ", [0, 3, 4], ids=["occ-default", "occ-3", "occ-4"])
 def test_batched_equals_plain(cuda, workloads, combo, order, occ):
     b, p, q, want = workloads["clustered"]
     ix = make_index(combo, sort_queries=order, query_occupancy=occ)
