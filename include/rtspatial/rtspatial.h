@@ -2,6 +2,7 @@
 #ifndef RTSPATIAL_B200_RTSPATIAL_H
 #define RTSPATIAL_B200_RTSPATIAL_H
 #include "rtspatial/geom/envelope.cuh"
+#include "rtspatial/geom/line.cuh"
 #include "rtspatial/geom/point.cuh"
 #include "rtspatial/spatial_index.cuh"
 #include "rtspatial/utils/queue.h"

@@ -21,6 +21,7 @@
 #include <type_traits>
 
 #include "rtspatial/geom/envelope.cuh"
+#include "rtspatial/geom/line.cuh"
 #include "rtspatial/geom/point.cuh"
 #include "rtspatial/geom/predicates.h"
 #include "rtspatial/utils/array_view.h"
@@ -74,6 +75,7 @@ class SpatialIndex {
  public:
   using point_t = Point<COORD_T, N_DIMS>;
   using envelope_t = Envelope<point_t>;
+  using line_t = Line<point_t>;
 
   SpatialIndex() = default;
   SpatialIndex(const SpatialIndex&) = delete;
@@ -171,6 +173,21 @@ class SpatialIndex {
                                     reinterpret_cast<const float*>(queries.data()),
                                     queries.size(), config_.handler, arg, stream));
     }
+  }
+
+  // Line queries (spatial_index.cuh:517-558).  The reference accepts them but
+  // reports no pair: kContains launches nothing and the kIntersects
+  // intersection program has its body commented out
+  // (src/shaders/shaders_intersects_line_query_2d.cu:14-41).  Same here: the
+  // call is checked and returns with no results.
+  void Query(Predicate p, ArrayView<line_t> queries, void* arg,
+             cudaStream_t stream = nullptr) {
+    (void)queries;
+    (void)arg;
+    (void)stream;
+    if (p != Predicate::kContains && p != Predicate::kIntersects)
+      throw Exception("unknown predicate");
+    handle();
   }
 
   size_t size() const { return h_ ? rts_size(h_) : 0; }

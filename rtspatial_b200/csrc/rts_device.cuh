@@ -380,16 +380,6 @@ struct QueryOps<kIntersects64> {
   static __device__ __forceinline__ bool node(float4 e, const Q& q) { return overlaps(e, q.nb); }
 };
 
-// Two consecutive boxes with one 32-byte read-only load (sm_100 256-bit
-// vector load): p must be 32-byte aligned.  Every W-group of the index starts
-// at a multiple of 16 W bytes from a 512-byte aligned base, so pairs (2c,
-// 2c+1) of a group are.
-__device__ __forceinline__ void ldg_box_pair(const float4* p, float4& a, float4& b) {
-  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
-      : "l"(p));
-}
-
 // ---------------------------------------------------------------------------
 // Per-level child masks of one traversal, packed W bits per level.
 // ---------------------------------------------------------------------------

@@ -293,6 +293,26 @@ TEST_CASE(PointQueries, fp64_contains_point_large_batch) {
   EXPECT_EQ_OR_FAIL(counter().get(s.cuda_stream()), 4224111ull);
 }
 
+// Line queries: the reference's kIntersects line shader reports nothing (its
+// intersection body is commented out), so neither does the drop-in.
+TEST_CASE(LineQueries, fp32_line_query_reports_like_the_reference) {
+  using line_t = index_t::line_t;
+  thrust::device_vector<envelope_t> env = uniform_boxes(10000, 0.5, 0.5);
+  std::vector<line_t> lh = {line_t(point_t(0, 0), point_t(1, 1)),
+                            line_t(point_t(0.5, 0), point_t(0.5, 1))};
+  thrust::device_vector<line_t> lines = lh;
+  Stream s;
+  Config config;
+  index_t index;
+  index.Init(config);
+  index.Insert(ArrayView<envelope_t>(env), s.cuda_stream());
+  for (Predicate p : {Predicate::kIntersects, Predicate::kContains}) {
+    counter().set(s.cuda_stream(), 0);
+    index.Query(p, ArrayView<line_t>(lines), counter().data(), s.cuda_stream());
+    EXPECT_EQ_OR_FAIL(counter().get(s.cuda_stream()), 0ull);
+  }
+}
+
 }  // namespace
 
 int main() {

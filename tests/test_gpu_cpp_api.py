@@ -19,4 +19,4 @@ def test_cpp_dropin_api(cuda):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert re.search(r"\b(\d+) tests, 0 failed", r.stdout), r.stdout
-    assert int(re.search(r"\b(\d+) tests, 0 failed", r.stdout).group(1)) >= 11
+    assert int(re.search(r"\b(\d+) tests, 0 failed", r.stdout).group(1)) >= 12
