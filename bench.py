@@ -573,11 +573,17 @@ def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1)
         return 1
     packet = cfg.traversal == 4 or (cfg.traversal == 0 and pred == 0)   # 0 = kIntersects
     merged = nbatch > 1 and cfg.traversal not in (2, 3) and (handler == 0 or packet)
-    end_bit = 32
-    while not merged and end_bit < 64 and (1 << (end_bit - 32)) < nbatch:
-        end_bit += 1
+    lg = 0
+    while lg < 40 and (1 << lg) < nq:
+        lg += 1
+    curve_bits = 2 * min(16, (lg + 1) // 2 + 2)      # order_curve_bits in rts_build.cu
+    bbits = 0
+    while not merged and (1 << bbits) < nbatch:
+        bbits += 1
+    passes = (curve_bits + bbits + 7) // 8
     chunk_order = nbatch > 1 and not merged and cfg.traversal != 3
-    return 1 + 1 + 2 + (end_bit + 7) // 8 + (1 if merged else 0) + (7 if chunk_order else 0)
+    chunk_kernels = 1 + 2 + (curve_bits + 7) // 8 if chunk_order else 0
+    return 1 + 1 + 2 + passes + (1 if merged else 0) + chunk_kernels
 
 
 def run_mutable_bench(args, ctx):

@@ -4,6 +4,7 @@
 // leaves sorted along a Morton or Hilbert curve of the box centres, grouped W
 // at a time, and W-wide upper levels computed as hulls of consecutive
 // entries.
+#include <algorithm>
 #include <cub/device/device_radix_sort.cuh>
 
 #include "rts_internal.h"
@@ -273,7 +274,7 @@ __device__ __forceinline__ uint32_t batch_of_query(const BatchDesc* descs, uint3
 __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDesc b0, uint32_t nb,
                              uint64_t total, const float4* __restrict__ frame_box, int curve,
                              unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals,
-                             bool merged) {
+                             bool merged, int curve_bits) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const uint32_t b = batch_of_query(descs, nb, i);
@@ -296,7 +297,8 @@ __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDes
   uint32_t qx = __float2uint_rz(fminf(fmaxf((c.x - f.x) * sx, 0.0f), 65535.0f));
   uint32_t qy = __float2uint_rz(fminf(fmaxf((c.y - f.y) * sy, 0.0f), 65535.0f));
   uint32_t k = (curve == RTS_CURVE_HILBERT) ? hilbert16(qx, qy) : (spread16(qx) | (spread16(qy) << 1));
-  keys[i] = merged ? k : (static_cast<unsigned long long>(b) << 32) | k;
+  k >>= 32 - curve_bits;  // the curve at 2^(curve_bits/2) cells per axis
+  keys[i] = merged ? k : (static_cast<unsigned long long>(b) << curve_bits) | k;
   vals[i] = merged ? static_cast<uint32_t>(i) : local;
 }
 
@@ -306,7 +308,7 @@ __global__ void k_query_keys(const BatchDesc* __restrict__ descs, const BatchDes
 // it makes the chunks in flight, whatever their batch, neighbours in space.
 __global__ void k_chunk_keys(const BatchDesc* __restrict__ descs, uint32_t nb,
                              uint32_t total_chunks, uint32_t chunk,
-                             const unsigned long long* __restrict__ sorted_keys,
+                             const unsigned long long* __restrict__ sorted_keys, uint32_t curve_mask,
                              uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (c >= total_chunks) return;
@@ -317,7 +319,7 @@ __global__ void k_chunk_keys(const BatchDesc* __restrict__ descs, uint32_t nb,
   }
   const BatchDesc& B = descs[lo];
   const uint64_t pos = B.qbase + static_cast<uint64_t>(c - B.chunk_begin) * chunk;
-  keys[c] = static_cast<uint32_t>(sorted_keys[pos]);
+  keys[c] = static_cast<uint32_t>(sorted_keys[pos]) & curve_mask;
   vals[c] = static_cast<uint32_t>(c);
 }
 
@@ -444,6 +446,19 @@ int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_
 }
 
 
+int order_curve_bits(uint64_t total) {
+  int lg = 0;
+  while (lg < 40 && (1ull << lg) < total) ++lg;
+  const int axis = std::min(16, (lg + 1) / 2 + 2);  // about 16 cells per query
+  return 2 * axis;
+}
+
+static int order_end_bit(uint64_t total, uint32_t nb, bool merged) {
+  int bbits = 0;
+  while (!merged && bbits < 32 && (1ull << bbits) < nb) ++bbits;
+  return order_curve_bits(total) + bbits;
+}
+
 int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
                        const float4* frame_box, int curve, unsigned long long* keys_a,
                        unsigned long long* keys_b, uint32_t* vals_a, uint32_t* order,
@@ -452,10 +467,9 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
   if (total == 0) return RTS_OK;
   merged = merged && nb > 1;
   k_query_keys<<<grid_for(total), kThreads, 0, s>>>(descs, b0, nb, total, frame_box, curve, keys_a,
-                                                    vals_a, merged);
+                                                    vals_a, merged, order_curve_bits(total));
   RTS_CUDA_TRY(cudaGetLastError());
-  int end_bit = 32;
-  while (!merged && end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
+  const int end_bit = order_end_bit(total, nb, merged);
   size_t need = 0;
   RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, keys_a, keys_b, vals_a, order,
                                                 static_cast<int>(total), 0, end_bit, s));
@@ -474,19 +488,22 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
 }
 
 int launch_chunk_order(const BatchDesc* descs, uint32_t nb, uint32_t total_chunks, uint32_t chunk,
-                       const unsigned long long* sorted_keys, uint32_t* keys_a, uint32_t* keys_b,
-                       uint32_t* vals_a, uint32_t* order, DevBuf& temp, cudaStream_t s) {
+                       uint64_t total, const unsigned long long* sorted_keys, uint32_t* keys_a,
+                       uint32_t* keys_b, uint32_t* vals_a, uint32_t* order, DevBuf& temp,
+                       cudaStream_t s) {
   if (total_chunks == 0 || nb < 2) return RTS_OK;
+  const int cbits = order_curve_bits(total);
+  const uint32_t mask = cbits >= 32 ? 0xffffffffu : ((1u << cbits) - 1u);
   k_chunk_keys<<<grid_for(total_chunks), kThreads, 0, s>>>(descs, nb, total_chunks, chunk,
-                                                           sorted_keys, keys_a, vals_a);
+                                                           sorted_keys, mask, keys_a, vals_a);
   RTS_CUDA_TRY(cudaGetLastError());
   size_t need = 0;
   RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, keys_a, keys_b, vals_a, order,
-                                                static_cast<int>(total_chunks), 0, 32, s));
+                                                static_cast<int>(total_chunks), 0, cbits, s));
   int rc = buf_reserve(temp, need, s, false, 0);
   if (rc) return rc;
   RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.ptr, need, keys_a, keys_b, vals_a, order,
-                                                static_cast<int>(total_chunks), 0, 32, s));
+                                                static_cast<int>(total_chunks), 0, cbits, s));
   return RTS_OK;
 }
 
@@ -500,8 +517,7 @@ int chunk_order_temp_bytes(uint32_t total_chunks, size_t* bytes) {
 }
 
 int query_order_temp_bytes(uint64_t total, uint32_t nb, size_t* bytes) {
-  int end_bit = 32;
-  while (end_bit < 64 && (1ull << (end_bit - 32)) < nb) ++end_bit;
+  const int end_bit = order_end_bit(total, nb, false);  // a merged order uses fewer bits
   *bytes = 0;
   RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(
       nullptr, *bytes, static_cast<const unsigned long long*>(nullptr),

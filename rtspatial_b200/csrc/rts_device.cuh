@@ -192,6 +192,22 @@ __device__ __forceinline__ bool isect_leaf(float4 g, const IsectQuery& Q) {
   return isect_exact(g, Q);
 }
 
+// isect_leaf for a stored box g tested against many queries: its hull h is
+// computed once, and its diagonal reciprocals the first time a query passes
+// the prefilter (gix, giy, have carry them between calls).  The same
+// operations as isect_leaf, so the same results.
+__device__ __forceinline__ bool isect_leaf_pre(float4 g, float4 h, float& gix, float& giy,
+                                               bool& have, const IsectQuery& Q) {
+  if (!overlaps(h, Q.nb)) return false;
+  if (!have) {
+    gix = __frcp_rn(__fsub_rn(g.z, g.x));
+    giy = __frcp_rn(__fsub_rn(g.w, g.y));
+    have = true;
+  }
+  if (slab_hit(g.x, g.y, gix, giy, Q.q)) return g.x < g.z && g.y < g.w;
+  return slab_hit(Q.ox, Q.oy, Q.invx, Q.invy, g);
+}
+
 // Magnitude bound of a tree from its root box (node boxes are hulls).
 __device__ __forceinline__ float2 root_magnitude(float4 r) {
   return make_float2(fmaxf(fabsf(r.x), fabsf(r.z)), fmaxf(fabsf(r.y), fabsf(r.w)));
@@ -416,32 +432,6 @@ struct MaskStack {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
-// Appends, for every lane, the pairs (ids[c], qid) for each set bit c of m.
-// Must be called by all 32 lanes.  One atomicAdd per warp; the queue's
-// counter keeps counting past capacity so the caller can see the size needed.
-__device__ __forceinline__ void collect_warp(const DevQueue& qu, uint32_t m,
-                                             const uint32_t* ids, uint32_t qid) {
-  const uint32_t lane = lane_id();
-  uint32_t cnt = __popc(m);
-  uint32_t incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t v = __shfl_up_sync(kFull, incl, o);
-    if (lane >= static_cast<uint32_t>(o)) incl += v;
-  }
-  uint32_t total = __shfl_sync(kFull, incl, 31);
-  if (total == 0) return;
-  uint32_t base = 0;
-  if (lane == 31) base = atomicAdd(qu.size, total);
-  base = __shfl_sync(kFull, base, 31);
-  unsigned long long p = static_cast<unsigned long long>(base) + (incl - cnt);
-  while (m) {
-    int c = __ffs(m) - 1;
-    m &= m - 1;
-    if (p < qu.capacity) qu.data[p] = DevPair{ids[c], qid};
-    ++p;
-  }
-}
 
 // Parameters of one batch (one reference Query call).
 struct BatchDesc {
@@ -471,6 +461,23 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
+}
+
+// Warp exclusive prefix sum (and total) of per-lane counts below 2^kBits,
+// from one ballot per bit: the ballots are independent, unlike the dependent
+// chain of a shuffle scan.
+template <int kBits>
+__device__ __forceinline__ uint32_t warp_excl_prefix(uint32_t cnt, uint32_t& total) {
+  const uint32_t lt = lanemask_lt();
+  uint32_t excl = 0;
+  total = 0;
+#pragma unroll
+  for (int b = 0; b < kBits; ++b) {
+    const uint32_t v = __ballot_sync(kFull, (cnt >> b) & 1u);
+    excl += static_cast<uint32_t>(__popc(v & lt)) << b;
+    total += static_cast<uint32_t>(__popc(v)) << b;
+  }
+  return excl;
 }
 
 // Counting handler of a merged launch: adds one finished query's count to
@@ -591,14 +598,9 @@ struct WarpOut {
                                       uint32_t qid, uint32_t rb) {
     if (!__any_sync(kFull, m != 0)) return;
     const uint32_t lane = lane_id();
-    uint32_t cnt = __popc(m);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t v = __shfl_up_sync(kFull, incl, o);
-      if (lane >= static_cast<uint32_t>(o)) incl += v;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t cnt = __popc(m);
+    uint32_t total;
+    const uint32_t excl = warp_excl_prefix<(W >= 32 ? 6 : W >= 16 ? 5 : W >= 8 ? 4 : 3)>(cnt, total);
     if (n + total > kWarpOutCap) flush(qu);
     if (ROUTED && total > kWarpOutCap) {  // more than a buffer, merged launch
       if (cnt) {
@@ -619,7 +621,7 @@ struct WarpOut {
       uint32_t base = 0;
       if (lane == 31) base = atomicAdd(qu.size, total);
       base = __shfl_sync(kFull, base, 31);
-      const unsigned long long p0 = static_cast<unsigned long long>(base) + (incl - cnt);
+      const unsigned long long p0 = static_cast<unsigned long long>(base) + excl;
 #pragma unroll
       for (int c = 0; c < W; ++c) {
         if ((m >> c) & 1u) {
@@ -629,14 +631,10 @@ struct WarpOut {
       }
       return;
     }
-    const uint32_t at = n + incl - cnt;
-#pragma unroll
-    for (int c = 0; c < W; ++c) {
-      if ((m >> c) & 1u) {
-        const uint32_t k = at + __popc(m & ((1u << c) - 1u));
-        buf[k] = DevPair{slot0 + c, qid};
-        if constexpr (ROUTED) bat[k] = rb;
-      }
+    uint32_t k = n + excl;
+    for (uint32_t mm = m; mm; mm &= mm - 1, ++k) {  // the set bits, lowest first
+      buf[k] = DevPair{slot0 + __ffs(mm) - 1, qid};
+      if constexpr (ROUTED) bat[k] = rb;
     }
     n += total;
   }
@@ -648,13 +646,8 @@ struct WarpOut {
     if (!__any_sync(kFull, hm != 0)) return;
     const uint32_t lane = lane_id();
     const uint32_t cnt = __popc(hm);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t v = __shfl_up_sync(kFull, incl, o);
-      if (lane >= static_cast<uint32_t>(o)) incl += v;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    uint32_t total;
+    const uint32_t excl = warp_excl_prefix<6>(cnt, total);
     if (n + total > kWarpOutCap) flush(qu);
     if (total > kWarpOutCap) {  // more than a buffer: straight to the queues
       if (hm == 0) return;
@@ -678,7 +671,7 @@ struct WarpOut {
       }
       return;
     }
-    uint32_t k = n + incl - cnt;
+    uint32_t k = n + excl;
     while (hm) {
       const uint32_t j = __ffs(hm) - 1;
       hm &= hm - 1;

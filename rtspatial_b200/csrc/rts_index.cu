@@ -355,7 +355,7 @@ int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
                             host[0].mode == kCollect ? static_cast<DevQueue*>(qs.m_routes.ptr)
                                                      : nullptr);
   if (rc || !plan.chunk_order) return rc;
-  return launch_chunk_order(dev, nd, static_cast<uint32_t>(chunks), plan.chunk,
+  return launch_chunk_order(dev, nd, static_cast<uint32_t>(chunks), plan.chunk, total,
                             static_cast<const unsigned long long*>(qs.keys_b.ptr),
                             static_cast<uint32_t*>(qs.ck_keys_a.ptr),
                             static_cast<uint32_t*>(qs.ck_keys_b.ptr),

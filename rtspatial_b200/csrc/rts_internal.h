@@ -85,8 +85,12 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
 // order = chunk ids sorted by the curve key of each chunk's first query
 // (sorted_keys = the sorted query keys the order sort left in keys_b).
 int launch_chunk_order(const BatchDesc* descs, uint32_t nb, uint32_t total_chunks, uint32_t chunk,
-                       const unsigned long long* sorted_keys, uint32_t* keys_a, uint32_t* keys_b,
-                       uint32_t* vals_a, uint32_t* order, DevBuf& temp, cudaStream_t s);
+                       uint64_t total, const unsigned long long* sorted_keys, uint32_t* keys_a,
+                       uint32_t* keys_b, uint32_t* vals_a, uint32_t* order, DevBuf& temp,
+                       cudaStream_t s);
+// Curve bits of the visiting-order keys of a launch of `total` queries
+// (the curve at about 16 cells per query, at most 16 bits per axis).
+int order_curve_bits(uint64_t total);
 int chunk_order_temp_bytes(uint32_t total_chunks, size_t* bytes);
 // Temporary bytes the order sort of `total` queries in `nb` batches needs
 // (an upper bound for the merged sort too).
