@@ -16,8 +16,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librtspatial_b200.so")
-SOURCES = ["rts_index.cu", "rts_plan.cu", "rts_server.cu", "rts_tune.cu", "rts_frontier.cu", "rts_query.cu", "rts_build.cu"]
-HEADERS = ["rts_device.cuh", "rts_traverse.cuh", "rts_internal.h", "rts_index_impl.h"]
+SOURCES = ["rts_query_occ1.cu", "rts_query_occ2.cu", "rts_query_occ3.cu", "rts_query_occ4.cu",
+           "rts_index.cu", "rts_plan.cu", "rts_server.cu", "rts_tune.cu", "rts_frontier.cu",
+           "rts_query.cu", "rts_build.cu"]
+HEADERS = ["rts_device.cuh", "rts_traverse.cuh", "rts_query_kernels.cuh", "rts_internal.h",
+           "rts_index_impl.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -55,7 +58,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd.insert(1, "-Xptxas=-v")
         cmds.append(cmd)
         objs.append(obj)
-    # one nvcc per source, in parallel (the query kernels dominate)
+    # one nvcc per source, in parallel (the query kernels, one source per
+    # occupancy, dominate)
     with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
         for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
             f.result()

@@ -26,6 +26,19 @@ __device__ __forceinline__ float ord2f(uint32_t o) {
   return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
 
+// Empty slot (padding, or a slot whose envelope moved to another sub-tree):
+// NaN in every coordinate fails each comparison of every predicate, so it
+// answers no query, even ones with infinite coordinates, and fminf / fmaxf
+// leave it out of node hulls.
+__device__ __forceinline__ float4 empty_box() {
+  return make_float4(__int_as_float(0x7fffffff), __int_as_float(0x7fffffff),
+                     __int_as_float(0x7fffffff), __int_as_float(0x7fffffff));
+}
+__device__ __forceinline__ DBox empty_dbox() {
+  const double n = __longlong_as_double(0x7fffffffffffffffll);
+  return DBox{make_double2(n, n), make_double2(n, n)};
+}
+
 __device__ __forceinline__ float4 hull(float4 b) {
   return make_float4(fminf(b.x, b.z), fminf(b.y, b.w), fmaxf(b.x, b.z), fmaxf(b.y, b.w));
 }
@@ -128,9 +141,8 @@ __global__ void k_fill_pad(float4* __restrict__ leaves, uint32_t* __restrict__ i
                            uint64_t to, DBox* __restrict__ leaves64) {
   uint64_t i = from + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= to) return;
-  leaves[i] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
-  if (leaves64)
-    leaves64[i] = DBox{make_double2(INFINITY, INFINITY), make_double2(-INFINITY, -INFINITY)};
+  leaves[i] = empty_box();
+  if (leaves64) leaves64[i] = empty_dbox();
   if (ids) ids[i] = 0xffffffffu;
 }
 
@@ -239,9 +251,8 @@ __global__ void k_update_apply(const E* __restrict__ upd, uint64_t n, uint64_t n
     return;
   }
   if (atomicOr(claimed + (slot >> 5), bit) & bit) return;  // another update moves this id
-  leaves[slot] = make_float4(INFINITY, INFINITY, -INFINITY, -INFINITY);
-  if (leaves64)
-    leaves64[slot] = DBox{make_double2(INFINITY, INFINITY), make_double2(-INFINITY, -INFINITY)};
+  leaves[slot] = empty_box();
+  if (leaves64) leaves64[slot] = empty_dbox();
   const uint32_t k = atomicAdd(n_moved, 1u);
   moved_ids[k] = static_cast<uint32_t>(e.id);
   moved[k] = b;

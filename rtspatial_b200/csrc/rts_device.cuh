@@ -154,6 +154,9 @@ __device__ __forceinline__ IsectQuery make_isect_query(float4 q) {
 // directions give infinite or NaN slab values, which only accept when the
 // origin lies within the slab.  The margin 2^-17*M + 2^-120 = (128u)*M + tiny
 // exceeds the bound with room for the rounding of the inflated bounds.
+// The bound needs finite coordinates: with an infinite one in the query or
+// the tree (M infinite), or a NaN in the query, the window is the whole
+// plane and the exact leaf test alone decides.
 // mag = per-axis magnitude bound of the tree's boxes.
 __device__ __forceinline__ void isect_set_margin(IsectQuery& Q, float2 mag) {
   const float4 q = Q.q;
@@ -165,6 +168,9 @@ __device__ __forceinline__ void isect_set_margin(IsectQuery& Q, float2 mag) {
   Q.nb.y = __fsub_rn(fminf(q.y, q.w), ey);
   Q.nb.z = __fadd_rn(fmaxf(q.x, q.z), ex);
   Q.nb.w = __fadd_rn(fmaxf(q.y, q.w), ey);
+  const bool finite = ex < INFINITY && ey < INFINITY && q.x == q.x && q.y == q.y &&
+                      q.z == q.z && q.w == q.w;
+  if (!finite) Q.nb = make_float4(-INFINITY, -INFINITY, INFINITY, INFINITY);
 }
 
 // Closed overlap of a (hull) box with the inflated query box.

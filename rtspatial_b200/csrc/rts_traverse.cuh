@@ -347,31 +347,59 @@ __device__ __forceinline__ void run_chunk_packet(const Forest& F, const BatchDes
         const bool valid = c < lim;
         uint32_t hm = 0;
         uint32_t rm = qm;
-        DBox g64{};          // double index: this entry's double envelope, loaded
-        bool have64 = false;  // the first time a query passes the float test
-        while (rm) {  // uniform: kGroups queries per round
-          uint32_t mine = rm;
-#pragma unroll
-          for (uint32_t k = 0; k + 1 < kGroups; ++k)
-            if (k < part) mine &= mine - 1;
-#pragma unroll
-          for (uint32_t k = 0; k < kGroups; ++k) rm &= rm - 1;
-          if (mine && valid) {
-            const uint32_t j = __ffs(mine) - 1;
-            bool hit;
-            if constexpr (Ops::kNeeds64) {
-              hit = at_leaf ? Ops::coarse(e, P.q[j]) : Ops::node(e, P.q[j]);
-              if (hit && at_leaf) {
-                if (!have64) {
-                  g64 = load_dbox(T.leaves64 + first + c);
-                  have64 = true;
-                }
-                hit = Ops::exact64(g64, P.q[j]);
+        // Per entry, prepared once for all the packet's queries: the hull of
+        // a stored box (the intersects prefilter), its diagonal reciprocals
+        // and (double index) its double envelope, the last two on first use.
+        const float4 eh =
+            make_float4(fminf(e.x, e.z), fminf(e.y, e.w), fmaxf(e.x, e.z), fmaxf(e.y, e.w));
+        float gix = 0.f, giy = 0.f;
+        bool have_rcp = false;
+        DBox g64{};
+        bool have64 = false;
+        auto test = [&](uint32_t j) -> bool {
+          if constexpr (Ops::kNeeds64) {
+            bool hit = at_leaf ? overlaps(eh, P.q[j].nb) : Ops::node(e, P.q[j]);
+            if (hit && at_leaf) {
+              if (!have64) {
+                g64 = load_dbox(T.leaves64 + first + c);
+                have64 = true;
               }
-            } else {
-              hit = at_leaf ? Ops::leaf(e, P.q[j]) : Ops::node(e, P.q[j]);
+              hit = Ops::exact64(g64, P.q[j]);
             }
-            if (hit) hm |= 1u << j;
+            return hit;
+          } else if constexpr (PRED == kIntersects) {
+            return at_leaf ? isect_leaf_pre(e, eh, gix, giy, have_rcp, P.q[j])
+                           : Ops::node(e, P.q[j]);
+          } else {
+            return at_leaf ? Ops::leaf(e, P.q[j]) : Ops::node(e, P.q[j]);
+          }
+        };
+        if constexpr (kGroups == 1) {
+          while (rm) {  // uniform: two queries per round
+            const uint32_t j1 = __ffs(rm) - 1;
+            rm &= rm - 1;
+            uint32_t j2 = 32;
+            if (rm) {
+              j2 = __ffs(rm) - 1;
+              rm &= rm - 1;
+            }
+            if (valid) {
+              if (test(j1)) hm |= 1u << j1;
+              if (j2 < 32 && test(j2)) hm |= 1u << j2;
+            }
+          }
+        } else {
+          while (rm) {  // uniform: kGroups queries per round
+            uint32_t mine = rm;
+#pragma unroll
+            for (uint32_t k = 0; k + 1 < kGroups; ++k)
+              if (k < part) mine &= mine - 1;
+#pragma unroll
+            for (uint32_t k = 0; k < kGroups; ++k) rm &= rm - 1;
+            if (mine && valid) {
+              const uint32_t j = __ffs(mine) - 1;
+              if (test(j)) hm |= 1u << j;
+            }
           }
         }
 #pragma unroll

@@ -162,6 +162,31 @@ def test_double_server(cuda, oracle, scene):
     sv.close()
 
 
+@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET])
+def test_double_emptied_slots_match_no_query(cuda, oracle, scene, t):
+    # Slots emptied by updates that move envelopes to a new sub-tree answer
+    # nothing, including queries with infinite coordinates.
+    boxes, pts, qs = scene
+    rng = np.random.default_rng(66)
+    ix = make(16, t, max_trees=8, rebuild_update_fraction=0.9)
+    ix.Insert(ddev(boxes))
+    far = rng.choice(boxes.shape[0], 1000, replace=False)
+    c = rng.random((far.shape[0], 2))
+    nb = np.concatenate([c, c + 0.01], axis=1)
+    ix.Update(torch.from_numpy(far.astype(np.int64)).cuda(), ddev(nb))
+    assert ix.num_trees() == 2
+    cur = boxes.copy()
+    cur[far] = nb
+    inf = np.inf
+    xq = np.concatenate([[[inf, inf, -inf, -inf], [-inf, -inf, inf, inf], [inf, inf, inf, inf],
+                          [inf, -inf, -inf, inf]], qs[:500]])
+    xp = np.concatenate([[[inf, inf], [-inf, -inf]], pts[:500]])
+    for kind, src in (("point", xp), ("contains", xq), ("intersects", xq)):
+        want = oracle.run64(KINDS[kind][0], cur, src)[2]
+        assert_same_pairs(canon(ix.query_pairs(KINDS[kind][1], ddev(src))), want, kind)
+        assert ix.query_count(KINDS[kind][1], ddev(src)) == want.shape[0]
+
+
 def test_double_and_float_calls_do_not_mix(cuda):
     ix = make(16, L.RTS_TRAVERSAL_AUTO)
     with pytest.raises(Exception):

@@ -127,6 +127,45 @@ def test_update_moves_far_envelopes_to_a_new_subtree(cuda, oracle, w, t):
     check_all(ix2, oracle, cur2, pts, qs, "after re-sort")
 
 
+@pytest.mark.parametrize("w,t", [(16, rb._lib.RTS_TRAVERSAL_THREAD), (32, rb._lib.RTS_TRAVERSAL_PACKET),
+                                 (8, rb._lib.RTS_TRAVERSAL_TEAM),
+                                 (8, rb._lib.RTS_TRAVERSAL_FRONTIER)],
+                         ids=["w16-thread", "w32-packet", "w8-team", "w8-frontier"])
+def test_emptied_slots_match_no_query(cuda, oracle, w, t):
+    # A slot emptied by a move keeps its id; it must not answer any query, not
+    # even the inverted infinite envelope that every stored box contains
+    # (closed-interval compares), nor infinite points and windows.
+    rng = np.random.default_rng(90 + w)
+    boxes = wl.uniform_boxes(rng, 5000, 5e-3)
+    ix = rb.SpatialIndex(rb.Config(node_width=w, traversal=t, max_trees=8,
+                                   rebuild_update_fraction=0.9))
+    ix.Insert(dev(boxes))
+    far = rng.choice(boxes.shape[0], 300, replace=False)
+    nb = wl.uniform_boxes(rng, far.shape[0], 5e-3)
+    ix.Update(torch.from_numpy(far.astype(np.int64)).cuda(), dev(nb))
+    assert ix.num_trees() == 2
+    cur = boxes.copy()
+    cur[far] = nb
+    inf = np.float32(np.inf)
+    qs = np.array([[inf, inf, -inf, -inf], [-inf, -inf, inf, inf], [inf, inf, inf, inf],
+                   [-inf, -inf, -inf, -inf], [0.2, 0.2, 0.21, 0.21], [inf, -inf, -inf, inf]],
+                  np.float32)
+    pts = np.array([[inf, inf], [-inf, -inf], [inf, -inf], [0.5, 0.5]], np.float32)
+    check_all(ix, oracle, cur, pts, qs, "extreme queries after moves")
+    for pred, kind, src in ((P.kContains, KIND_CONTAINS, qs), (P.kIntersects, KIND_INTERSECTS, qs),
+                            (P.kContains, KIND_POINT, pts)):
+        assert ix.query_count(pred, dev(src)) == oracle.run(kind, cur, src)[2].shape[0]
+    # stored envelopes with infinite coordinates (node hulls and the
+    # intersects margin become infinite)
+    wild = np.array([[-inf, 0.2, 0.3, 0.4], [0.1, 0.1, inf, inf], [-inf, -inf, inf, inf],
+                     [0.5, -inf, 0.5, inf]], np.float32)
+    ix.Insert(dev(wild))
+    cur = np.concatenate([cur, wild])
+    normal_qs = wl.uniform_boxes(rng, 500, 2e-2)
+    check_all(ix, oracle, cur, np.concatenate([pts, wl.uniform_points(rng, 500)]),
+              np.concatenate([qs, normal_qs]), "infinite stored envelopes")
+
+
 def test_update_listing_an_id_twice_keeps_one_envelope(cuda, oracle):
     rng = np.random.default_rng(17)
     boxes = wl.uniform_boxes(rng, 20_000, 5e-3)
