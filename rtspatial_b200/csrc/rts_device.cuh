@@ -42,6 +42,26 @@ __device__ __forceinline__ DBox load_dbox(const DBox* p) {
 }
 enum HandlerKind : int { kCount = 0, kCollect = 1 };
 
+// Two consecutive boxes with one 32-byte read-only load (sm_100 256-bit
+// vector load, four 64-bit lanes).  p must be 32-byte aligned: every W-group
+// starts 16 * W bytes after a multiple of 512 (sub-trees start on 32-slot
+// boundaries, node levels on W-entry ones), so the pairs (2c, 2c + 1) of a
+// group are; refresh_forest checks the buffers' bases.
+__device__ __forceinline__ void ldg_box_pair(const float4* p, float4& a, float4& b) {
+  unsigned long long x0, x1, x2, x3;
+  asm("ld.global.nc.v4.b64 {%0, %1, %2, %3}, [%4];"
+      : "=l"(x0), "=l"(x1), "=l"(x2), "=l"(x3)
+      : "l"(p));
+  a = make_float4(__uint_as_float(static_cast<uint32_t>(x0)),
+                  __uint_as_float(static_cast<uint32_t>(x0 >> 32)),
+                  __uint_as_float(static_cast<uint32_t>(x1)),
+                  __uint_as_float(static_cast<uint32_t>(x1 >> 32)));
+  b = make_float4(__uint_as_float(static_cast<uint32_t>(x2)),
+                  __uint_as_float(static_cast<uint32_t>(x2 >> 32)),
+                  __uint_as_float(static_cast<uint32_t>(x3)),
+                  __uint_as_float(static_cast<uint32_t>(x3 >> 32)));
+}
+
 struct TreeDesc {
   const float4* leaves;  // first slot of this tree
   const DBox* leaves64;  // double index: the double envelopes of the same slots

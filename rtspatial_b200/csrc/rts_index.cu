@@ -233,13 +233,13 @@ int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
 
 int refresh_forest(rts_index* ix) {
   if (!ix->forest_dirty) return RTS_OK;
-  // Every W-group is read as W 16-byte loads: the buffers the groups live in
-  // must start on a 16-byte boundary (device allocations start on 256-byte
-  // ones; this only guards that assumption).
-  const auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  // The thread scheme reads a W-group as W / 2 32-byte loads: the buffers the
+  // groups live in must start on a 32-byte boundary (device allocations start
+  // on 256-byte ones; this only guards that assumption).
+  const auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; };
   bool ok = aligned(ix->leaves.ptr);
   for (const auto& t : ix->trees) ok = ok && aligned(t.nodes.ptr);
-  if (!ok) return fail(RTS_ERR_CUDA, "index buffer not 16-byte aligned");
+  if (!ok) return fail(RTS_ERR_CUDA, "index buffer not 32-byte aligned");
   Forest& F = ix->forest;
   std::memset(&F, 0, sizeof(F));
   F.n_trees = static_cast<uint32_t>(ix->trees.size());

@@ -130,7 +130,7 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       const uint32_t lim = (at_leaf ? T.n : T.level_cnt[s.L]) - first;
       float4 e[W];
 #pragma unroll
-      for (int c = 0; c < W; ++c) e[c] = __ldg(p + c);
+      for (int c = 0; c < W; c += 2) ldg_box_pair(p + c, e[c], e[c + 1]);
       uint32_t m = 0;
 #pragma unroll
       for (int c = 0; c < W; ++c)
