@@ -552,10 +552,26 @@ struct WarpOut {
       uint32_t base = 0;
       if (lane_id() == 0) base = atomicAdd(qu.size, n);
       base = __shfl_sync(kFull, base, 0);
-      for (uint32_t i = lane_id(); i < n; i += 32) {
-        const DevPair e = buf[i];
-        unsigned long long p = static_cast<unsigned long long>(base) + i;
-        if (p < qu.capacity) qu.data[p] = DevPair{__ldg(ids + e.geom_id), e.query_id};
+      // Four rows of 32 at a time: their id loads are issued before any of
+      // their stores, so a flush waits for ceil(n / 128) id round trips.
+      constexpr int kRows = 4;
+      for (uint32_t i0 = 0; i0 < n; i0 += 32 * kRows) {
+        uint32_t gid[kRows], qid[kRows];
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+          const uint32_t i = i0 + lane_id() + 32u * r;
+          if (i < n) {
+            const DevPair e = buf[i];
+            gid[r] = __ldg(ids + e.geom_id);
+            qid[r] = e.query_id;
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+          const uint32_t i = i0 + lane_id() + 32u * r;
+          const unsigned long long p = static_cast<unsigned long long>(base) + i;
+          if (i < n && p < qu.capacity) qu.data[p] = DevPair{gid[r], qid[r]};
+        }
       }
     }
     __syncwarp();
