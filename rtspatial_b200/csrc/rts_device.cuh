@@ -674,9 +674,13 @@ struct WarpOut {
       return;
     }
     uint32_t k = n + excl;
-    for (uint32_t mm = m; mm; mm &= mm - 1, ++k) {  // the set bits, lowest first
-      buf[k] = DevPair{slot0 + __ffs(mm) - 1, qid};
-      if constexpr (ROUTED) bat[k] = rb;
+#pragma unroll
+    for (int c = 0; c < W; ++c) {  // the set bits, lowest first (predicated, no divergence)
+      if ((m >> c) & 1u) {
+        buf[k] = DevPair{slot0 + c, qid};
+        if constexpr (ROUTED) bat[k] = rb;
+        ++k;
+      }
     }
     n += total;
   }
