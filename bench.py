@@ -580,6 +580,8 @@ def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1)
     bbits = 0
     while not merged and (1 << bbits) < nbatch:
         bbits += 1
+    if bbits > 0 and curve_bits + bbits > 24:
+        curve_bits = max(16, min(curve_bits, (24 - bbits) & ~1))
     passes = (curve_bits + bbits + 7) // 8
     chunk_order = nbatch > 1 and not merged and cfg.traversal != 3
     chunk_kernels = 1 + 2 + (curve_bits + 7) // 8 if chunk_order else 0

@@ -457,17 +457,26 @@ int launch_pack_tree(const float4* leaves, const HostTree& t, int W, cudaStream_
 }
 
 
-int order_curve_bits(uint64_t total) {
+static int order_batch_bits(uint32_t nb, bool merged) {
+  int bbits = 0;
+  while (!merged && bbits < 32 && (1ull << bbits) < nb) ++bbits;
+  return bbits;
+}
+
+int order_curve_bits(uint64_t total, uint32_t nb, bool merged) {
   int lg = 0;
   while (lg < 40 && (1ull << lg) < total) ++lg;
-  const int axis = std::min(16, (lg + 1) / 2 + 2);  // about 16 cells per query
-  return 2 * axis;
+  int bits = 2 * std::min(16, (lg + 1) / 2 + 2);  // about 16 cells per query
+  // (batch, curve) keys of an unmerged launch: fit them in three 8-bit radix
+  // passes where that leaves at least 8 bits per axis (the curve orders
+  // queries within their own batch, which holds a share of the total).
+  const int bbits = order_batch_bits(nb, merged);
+  if (bbits > 0 && bits + bbits > 24) bits = std::max(16, std::min(bits, (24 - bbits) & ~1));
+  return bits;
 }
 
 static int order_end_bit(uint64_t total, uint32_t nb, bool merged) {
-  int bbits = 0;
-  while (!merged && bbits < 32 && (1ull << bbits) < nb) ++bbits;
-  return order_curve_bits(total) + bbits;
+  return order_curve_bits(total, nb, merged) + order_batch_bits(nb, merged);
 }
 
 int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb, uint64_t total,
@@ -478,7 +487,8 @@ int launch_query_order(const BatchDesc* descs, const BatchDesc& b0, uint32_t nb,
   if (total == 0) return RTS_OK;
   merged = merged && nb > 1;
   k_query_keys<<<grid_for(total), kThreads, 0, s>>>(descs, b0, nb, total, frame_box, curve, keys_a,
-                                                    vals_a, merged, order_curve_bits(total));
+                                                    vals_a, merged,
+                                                    order_curve_bits(total, nb, merged));
   RTS_CUDA_TRY(cudaGetLastError());
   const int end_bit = order_end_bit(total, nb, merged);
   size_t need = 0;
@@ -503,7 +513,7 @@ int launch_chunk_order(const BatchDesc* descs, uint32_t nb, uint32_t total_chunk
                        uint32_t* keys_b, uint32_t* vals_a, uint32_t* order, DevBuf& temp,
                        cudaStream_t s) {
   if (total_chunks == 0 || nb < 2) return RTS_OK;
-  const int cbits = order_curve_bits(total);
+  const int cbits = order_curve_bits(total, nb, false);  // as the unmerged query keys
   const uint32_t mask = cbits >= 32 ? 0xffffffffu : ((1u << cbits) - 1u);
   k_chunk_keys<<<grid_for(total_chunks), kThreads, 0, s>>>(descs, nb, total_chunks, chunk,
                                                            sorted_keys, mask, keys_a, vals_a);

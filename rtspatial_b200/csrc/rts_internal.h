@@ -88,9 +88,11 @@ int launch_chunk_order(const BatchDesc* descs, uint32_t nb, uint32_t total_chunk
                        uint64_t total, const unsigned long long* sorted_keys, uint32_t* keys_a,
                        uint32_t* keys_b, uint32_t* vals_a, uint32_t* order, DevBuf& temp,
                        cudaStream_t s);
-// Curve bits of the visiting-order keys of a launch of `total` queries
-// (the curve at about 16 cells per query, at most 16 bits per axis).
-int order_curve_bits(uint64_t total);
+// Curve bits of the visiting-order keys of a launch of `total` queries in
+// `nb` batches (the curve at about 16 cells per query, at most 16 bits per
+// axis; fewer, down to 8 per axis, so that an unmerged launch's (batch,
+// curve) keys fit in 24 bits).
+int order_curve_bits(uint64_t total, uint32_t nb, bool merged);
 int chunk_order_temp_bytes(uint32_t total_chunks, size_t* bytes);
 // Temporary bytes the order sort of `total` queries in `nb` batches needs
 // (an upper bound for the merged sort too).
