@@ -117,7 +117,8 @@ typedef struct rts_config {
   int32_t sort_queries;   /* visit queries in curve order (results keep the caller's query ids):
                              0 never, 1 always, 2 when a launch has >= 8192 queries */
   float rebuild_update_fraction; /* updates since the last rebuild, as a fraction of the index,
-                                    above which Update re-sorts instead of refitting */
+                                    above which Update re-sorts every box (below it, envelopes
+                                    are written in place or moved to a new sub-tree) */
   uint32_t chunk;         /* queries per device work item (0 = library default) */
   int32_t query_occupancy; /* 2 / 3 / 4: query kernel capped at 128 / 80 / 64 registers
                               (2 / 3 / 4 CTAs of 256 threads per SM); 1: uncapped; 0: per

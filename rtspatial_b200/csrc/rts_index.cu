@@ -6,8 +6,10 @@
 // IAS over all of them, spatial_index.cuh:142-196); after max_trees sub-trees,
 // or for a batch larger than rebuild_fraction of the index, all boxes are
 // re-sorted into a single tree.  Delete collapses boxes in place (node boxes
-// stay conservative, no refit needed); Update overwrites boxes and refits every
-// sub-tree, or re-sorts once the updates since the last rebuild exceed
+// stay conservative, no refit needed).  Update writes an envelope in place
+// when it stays inside its leaf group's hull; otherwise the slot is emptied
+// (a NaN box) and the envelope moves, with its id, into a new sub-tree.  All
+// boxes are re-sorted once the updates since the last rebuild exceed
 // rebuild_update_fraction of the index.
 #include <cuda_runtime.h>
 
