@@ -1,6 +1,6 @@
 """Benchmark of the hot path: SpatialIndex::Query on the B200 library.
 
-Default workload (the BASELINE metric's configuration that fits one GPU):
+Default workload (the headline configuration, the largest that fits one GPU):
 range-contains, float32 2-D, 10M boxes from 64 Gaussian clusters, 1M query
 boxes split into 256 log-uniform batches (1K-16K) run in ONE persistent
 launch (rts_query_batched), collecting handler (pairs written to per-batch
@@ -34,6 +34,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -137,7 +138,10 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        # the raw samples go to RTS_CLOCKS_DIR (default: the system temp dir);
+        # the JSON line carries their summary
+        out_dir = os.environ.get("RTS_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_rank{gpu_index}.csv")
 
     def start(self):
         try:
