@@ -125,7 +125,8 @@ __global__ void k_gather(const float4* __restrict__ src, const uint32_t* __restr
                          const uint32_t* __restrict__ order, uint64_t n, uint64_t id_begin,
                          uint64_t slot_base, float4* __restrict__ leaves,
                          uint32_t* __restrict__ leaf_ids, uint32_t* __restrict__ pos,
-                         const DBox* __restrict__ src64, DBox* __restrict__ leaves64) {
+                         const DBox* __restrict__ src64, DBox* __restrict__ leaves64,
+                         bool live_only) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t o = order[i];
@@ -134,7 +135,15 @@ __global__ void k_gather(const float4* __restrict__ src, const uint32_t* __restr
   leaves[slot] = src[o];
   if (leaves64) leaves64[slot] = src64[o];
   leaf_ids[slot] = id;
-  pos[id] = static_cast<uint32_t>(slot);
+  // An emptied slot (its envelope moved on) keeps a stale id: pos[id] points
+  // elsewhere and stays.  New slots lie past every source slot, so a stale
+  // copy never matches, whichever order the two copies' threads run in.
+  if (!live_only || pos[id] == o) pos[id] = static_cast<uint32_t>(slot);
+}
+
+__global__ void k_iota(uint32_t* __restrict__ out, uint64_t first, uint64_t n) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = static_cast<uint32_t>(first + i);
 }
 
 __global__ void k_fill_pad(float4* __restrict__ leaves, uint32_t* __restrict__ ids, uint64_t from,
@@ -420,10 +429,18 @@ int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_
 
 int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
                   uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
-                  uint32_t* pos, cudaStream_t s, const DBox* src64, DBox* leaves64) {
+                  uint32_t* pos, cudaStream_t s, const DBox* src64, DBox* leaves64,
+                  bool live_only) {
   if (n == 0) return RTS_OK;
   k_gather<<<grid_for(n), kThreads, 0, s>>>(src, src_ids, order, n, id_begin, slot_base, leaves,
-                                            leaf_ids, pos, src64, leaves64);
+                                            leaf_ids, pos, src64, leaves64, live_only);
+  RTS_CUDA_TRY(cudaGetLastError());
+  return RTS_OK;
+}
+
+int launch_iota(uint32_t* out, uint64_t first, uint64_t n, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  k_iota<<<grid_for(n), kThreads, 0, s>>>(out, first, n);
   RTS_CUDA_TRY(cudaGetLastError());
   return RTS_OK;
 }

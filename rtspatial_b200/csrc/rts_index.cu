@@ -5,8 +5,10 @@
 // sub-tree for the new batch (the reference builds one GAS per batch and an
 // IAS over all of them, spatial_index.cuh:142-196); after max_trees sub-trees,
 // or for a batch larger than rebuild_fraction of the index, all boxes are
-// re-sorted into a single tree.  Delete collapses boxes in place (node boxes
-// stay conservative, no refit needed).  Update writes an envelope in place
+// re-sorted into a single tree; at the sub-tree limit, sub-trees that are
+// small beside the largest are merged into one instead (merge_small_trees).
+// Delete collapses boxes in place (node boxes stay conservative, no refit
+// needed).  Update writes an envelope in place
 // when it stays inside its leaf group's hull; otherwise the slot is emptied
 // (a NaN box) and the envelope moves, with its id, into a new sub-tree.  All
 // boxes are re-sorted once the updates since the last rebuild exceed
@@ -137,7 +139,7 @@ int build_tree_levels(rts_index* ix, HostTree& t, cudaStream_t s) {
 int sort_into_slots(rts_index* ix, const float4* src, const uint32_t* src_ids, const uint32_t* idx,
                     uint64_t n, uint64_t id_begin, uint64_t slot_base, float4* dst_leaves,
                     uint32_t* dst_ids, cudaStream_t s, const DBox* src64 = nullptr,
-                    DBox* dst64 = nullptr) {
+                    DBox* dst64 = nullptr, bool live_only = false) {
   int rc = ensure_sort_scratch(ix, n, s);
   if (rc) return rc;
   auto* bounds = static_cast<uint32_t*>(ix->bounds.ptr);
@@ -149,7 +151,7 @@ int sort_into_slots(rts_index* ix, const float4* src, const uint32_t* src_ids, c
   if ((rc = launch_curve_keys(src, idx, n, bounds, ix->cfg.curve, ka, va, s))) return rc;
   if ((rc = sort_pairs(ka, kb, va, vb, n, ix->sort_temp, s))) return rc;
   if ((rc = launch_gather(src, src_ids, vb, n, id_begin, slot_base, dst_leaves, dst_ids,
-                          pos_of(ix), s, src64, dst64)))
+                          pos_of(ix), s, src64, dst64, live_only)))
     return rc;
   return launch_fill_pad(dst_leaves, dst_ids, slot_base + n, slot_base + round_up(n, kSlotAlign), s,
                          dst64);
@@ -230,6 +232,69 @@ int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
   ix->updated_since_build = 0;
   ix->forest_dirty = true;
   ix->version++;
+  return RTS_OK;
+}
+
+// Sub-tree limit reached: when every sub-tree but the largest together hold
+// at most an eighth as many slots as it, they are merged into one new sub-tree
+// behind the used slots and the largest stays as it is (the cost follows the
+// small trees, not the index).  Their slots are gathered whole: slots
+// emptied by moved updates come along as NaN boxes, which answer nothing, and
+// pos[] moves only for ids whose envelope a slot still holds.  The old slots
+// stay unused until the next full re-sort.  Beyond an eighth, queries would
+// walk a second large tree, and a full re-sort is due instead.
+static bool small_trees_mergeable(const rts_index* ix) {
+  const auto& tr = ix->trees;
+  if (tr.size() < 3 || ix->cfg.max_trees < 2) return false;
+  size_t big = 0;
+  for (size_t i = 1; i < tr.size(); ++i)
+    if (tr[i].n > tr[big].n) big = i;
+  if (big + 1 == tr.size()) return false;  // the newest tree (no levels yet) is the largest
+  uint64_t m = 0;
+  for (size_t i = 0; i < tr.size(); ++i)
+    if (i != big) m += tr[i].n;
+  const uint64_t end = ix->slot_end + round_up(m, kSlotAlign);
+  return 8 * m <= tr[big].n && end <= 2 * ix->n_ids + (1u << 20) && end < 0xffffffffull - kSlotAlign;
+}
+
+static int merge_small_trees(rts_index* ix, cudaStream_t s) {
+  auto& tr = ix->trees;
+  size_t big = 0;
+  for (size_t i = 1; i < tr.size(); ++i)
+    if (tr[i].n > tr[big].n) big = i;
+  uint64_t m = 0;
+  for (size_t i = 0; i < tr.size(); ++i)
+    if (i != big) m += tr[i].n;
+  const uint64_t base = ix->slot_end;
+  const uint64_t end = base + round_up(m, kSlotAlign);
+  int rc;
+  if ((rc = ensure_slots(ix, end, s))) return rc;
+  if ((rc = buf_reserve(ix->slots_tmp, std::max<uint64_t>(m, 1) * sizeof(uint32_t), s, false, 0)))
+    return rc;
+  auto* slots = static_cast<uint32_t*>(ix->slots_tmp.ptr);
+  uint64_t off = 0;
+  for (size_t i = 0; i < tr.size(); ++i) {
+    if (i == big) continue;
+    if ((rc = launch_iota(slots + off, tr[i].slot_base, tr[i].n, s))) return rc;
+    off += tr[i].n;
+  }
+  if ((rc = sort_into_slots(ix, leaves_of(ix), ids_of(ix), slots, m, 0, base, leaves_of(ix),
+                            ids_of(ix), s, leaves64_of(ix), leaves64_of(ix), true)))
+    return rc;
+  HostTree keep = tr[big];
+  for (size_t i = 0; i < tr.size(); ++i)
+    if (i != big) buf_free(tr[i].nodes, s);
+  tr.clear();
+  tr.push_back(keep);
+  HostTree t;
+  t.id_begin = 0;  // ids of several batches: read from leaf_ids
+  t.n = m;
+  t.slot_base = base;
+  ix->slot_end = end;
+  ix->forest_dirty = true;
+  ix->version++;
+  if ((rc = build_tree_levels(ix, t, s))) return rc;
+  tr.push_back(t);
   return RTS_OK;
 }
 
@@ -660,15 +725,16 @@ int insert_impl(rts_index* ix, const float4* src, const DBox* src64, const uint3
   t.id_begin = ids ? 0 : ix->n_ids;
   t.n = n;
   t.slot_base = slot_base;
-  const bool merge = !ix->trees.empty() &&
-                     (static_cast<int>(ix->trees.size()) >= ix->cfg.max_trees ||
-                      static_cast<double>(n) > ix->cfg.rebuild_fraction * static_cast<double>(ix->n_ids));
+  const bool big_batch = !ix->trees.empty() && static_cast<double>(n) >
+                                                  ix->cfg.rebuild_fraction * static_cast<double>(ix->n_ids);
+  const bool at_limit = !ix->trees.empty() && static_cast<int>(ix->trees.size()) >= ix->cfg.max_trees;
   if (!ids) ix->n_ids += n;
   ix->slot_end = slot_end;
   ix->forest_dirty = true;
   ix->version++;
-  if (merge) {
-    ix->trees.push_back(t);  // no levels yet; rebuild_all only reads its slots
+  if (big_batch || at_limit) {
+    ix->trees.push_back(t);  // no levels yet; a merge or re-sort only reads its slots
+    if (!big_batch && small_trees_mergeable(ix)) return merge_small_trees(ix, s);
     return rebuild_all(ix, s);
   }
   if ((rc = build_tree_levels(ix, t, s))) return rc;

@@ -59,12 +59,16 @@ int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_
                uint64_t n, DevBuf& temp, cudaStream_t s);
 // For i < n with o = order[i]: leaves[slot_base+i] = src[o];
 // id = src_ids ? src_ids[o] : id_begin + o; leaf_ids[slot_base+i] = id;
-// pos[id] = slot_base + i.  A double index also gathers src64 into leaves64.
+// pos[id] = slot_base + i (live_only: only where pos[id] == o, i.e. slot o
+// still holds id's envelope).  A double index also gathers src64 into
+// leaves64.
 int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
                   uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
                   uint32_t* pos, cudaStream_t s, const DBox* src64 = nullptr,
-                  DBox* leaves64 = nullptr);
-// Empty boxes (+inf, +inf, -inf, -inf) in slots [from, to); ids = ~0.
+                  DBox* leaves64 = nullptr, bool live_only = false);
+// out[i] = first + i for i < n.
+int launch_iota(uint32_t* out, uint64_t first, uint64_t n, cudaStream_t s);
+// Empty boxes (NaN) in slots [from, to); ids = ~0.
 int launch_fill_pad(float4* leaves, uint32_t* ids, uint64_t from, uint64_t to, cudaStream_t s,
                     DBox* leaves64 = nullptr);
 // Levels 1..top and the root box of a tree from its leaves.

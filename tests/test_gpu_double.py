@@ -187,6 +187,31 @@ def test_double_emptied_slots_match_no_query(cuda, oracle, scene, t):
         assert ix.query_count(KINDS[kind][1], ddev(src)) == want.shape[0]
 
 
+def test_double_small_subtrees_merge(cuda, oracle, scene):
+    # Sub-tree merges carry the double envelopes with their slots.
+    boxes, pts, qs = scene
+    rng = np.random.default_rng(67)
+    ix = make(16, L.RTS_TRAVERSAL_THREAD, max_trees=3, rebuild_fraction=0.5,
+              rebuild_update_fraction=0.9)
+    ix.Insert(ddev(boxes))
+    cur = boxes.copy()
+    for step in range(6):
+        if step % 2:
+            ids = rng.choice(cur.shape[0], 200, replace=False)
+            c = rng.random((ids.shape[0], 2))
+            nb = np.concatenate([c, c + 0.01], axis=1)
+            ix.Update(torch.from_numpy(ids.astype(np.int64)).cuda(), ddev(nb))
+            cur[ids] = nb
+        else:
+            new = boxes[rng.choice(boxes.shape[0], 500, replace=False)] + 1e-9
+            ix.Insert(ddev(new))
+            cur = np.concatenate([cur, new])
+        assert 2 <= ix.num_trees() <= 3
+    for kind, src in (("point", pts), ("contains", qs), ("intersects", qs)):
+        assert_same_pairs(canon(ix.query_pairs(KINDS[kind][1], ddev(src))),
+                          oracle.run64(KINDS[kind][0], cur, src)[2], kind)
+
+
 def test_double_and_float_calls_do_not_mix(cuda):
     ix = make(16, L.RTS_TRAVERSAL_AUTO)
     with pytest.raises(Exception):

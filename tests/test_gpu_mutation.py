@@ -166,6 +166,50 @@ def test_emptied_slots_match_no_query(cuda, oracle, w, t):
               np.concatenate([qs, normal_qs]), "infinite stored envelopes")
 
 
+@pytest.mark.parametrize("w,t", [(16, rb._lib.RTS_TRAVERSAL_THREAD), (32, rb._lib.RTS_TRAVERSAL_PACKET),
+                                 (8, rb._lib.RTS_TRAVERSAL_TEAM)], ids=["w16-thread", "w32-packet",
+                                                                        "w8-team"])
+def test_small_subtrees_merge_beside_the_base(cuda, oracle, w, t):
+    # At the sub-tree limit, sub-trees that are small beside the largest merge
+    # into one new sub-tree and the largest keeps its slots (no full re-sort:
+    # at least two sub-trees remain).  Slots emptied by moved updates come
+    # along into the merge; their ids must keep pointing at the live copies.
+    rng = np.random.default_rng(77 + w)
+    base = wl.uniform_boxes(rng, 120_000, 5e-3)
+    pts = wl.uniform_points(rng, 2000)
+    qs = wl.uniform_boxes(rng, 2000, 2e-2)
+    ix = rb.SpatialIndex(rb.Config(node_width=w, traversal=t, max_trees=4, rebuild_fraction=0.5,
+                                   rebuild_update_fraction=0.9))
+    ix.Insert(dev(base))
+    cur = base.copy()
+    merged_seen = False
+    for step in range(14):
+        before = ix.num_trees()
+        if step % 3 == 2:   # far moves: emptied slots plus a moved sub-tree
+            ids = rng.choice(cur.shape[0], 400, replace=False)
+            nb = wl.uniform_boxes(rng, ids.shape[0], 5e-3)
+            ix.Update(torch.from_numpy(ids.astype(np.int64)).cuda(), dev(nb))
+            cur[ids] = nb
+        else:
+            new = wl.uniform_boxes(rng, int(rng.integers(300, 1500)), 5e-3)
+            ix.Insert(dev(new))
+            cur = np.concatenate([cur, new])
+        if step % 4 == 3:   # deletes reach ids wherever they now live
+            dels = rng.choice(cur.shape[0], 300, replace=False)
+            ix.Delete(torch.from_numpy(dels.astype(np.int64)).cuda())
+            oracle.invalidate(cur, dels)
+        merged_seen |= ix.num_trees() < before
+        assert 2 <= ix.num_trees() <= 4, f"step {step}: {ix.num_trees()} sub-trees"
+        assert ix.size() == cur.shape[0]
+        check_all(ix, oracle, cur, pts, qs, f"step {step}")
+    assert merged_seen
+    # a full re-sort afterwards still finds every id once
+    ix2 = rb.SpatialIndex(rb.Config(node_width=w, traversal=t))
+    ix2.Insert(dev(cur))
+    for pred, src in ((P.kContains, pts), (P.kContains, qs), (P.kIntersects, qs)):
+        assert ix.query_count(pred, dev(src)) == ix2.query_count(pred, dev(src))
+
+
 def test_update_listing_an_id_twice_keeps_one_envelope(cuda, oracle):
     rng = np.random.default_rng(17)
     boxes = wl.uniform_boxes(rng, 20_000, 5e-3)
