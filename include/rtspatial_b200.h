@@ -112,7 +112,9 @@ typedef struct rts_config {
   int32_t node_width;     /* children per node and boxes per leaf: 4, 8, 16 or 32 (default 16) */
   int32_t traversal;      /* RTS_TRAVERSAL_* */
   int32_t curve;          /* RTS_CURVE_*: the order leaves are packed in */
-  int32_t max_trees;      /* insert batches kept as separate sub-trees before a merge rebuild (1..16) */
+  int32_t max_trees;      /* sub-trees kept before a merge (1..16): the sub-trees beside the
+                             largest merge into one when they hold at most an eighth of its
+                             slots, else every box is re-sorted into one tree */
   float rebuild_fraction; /* an insert batch larger than this fraction of the index rebuilds everything */
   int32_t sort_queries;   /* visit queries in curve order (results keep the caller's query ids):
                              0 never, 1 always, 2 when a launch has >= 8192 queries */
