@@ -13,8 +13,7 @@
 
 namespace rts {
 
-// Per-thread error message behind rts_last_error().
-void set_error(const std::string& msg);
+// Record the per-thread message behind rts_last_error() and return the code.
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
