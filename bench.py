@@ -1,22 +1,31 @@
 """Benchmark of the hot path: SpatialIndex::Query on the B200 library.
 
-Default workload (the headline configuration, the largest that fits one GPU):
-range-contains, float32 2-D, 10M boxes from 64 Gaussian clusters, 1M query
-boxes split into 256 log-uniform batches (1K-16K) run in ONE persistent
-launch (rts_query_batched), collecting handler (pairs written to per-batch
-device queues).  One step = all 256 batches once.
+Default workload (the headline: the configuration quoted as batched vs plain
+one-launch-per-batch): range-contains, float32 2-D, 10M boxes from 64
+Gaussian clusters, 1M query boxes split into 256 log-uniform batches
+(1K-16K) run in ONE persistent launch (rts_query_batched), collecting handler
+(pairs written to per-batch device queues).  One step = all 256 batches once.
 
 Printed on rank 0 as one JSON line:
   value        queries/s of the batched launch, inputs resident in HBM, L2
                flushed before every timed step (CUDA events per step)
-  plain        the same batches as 256 separate launches (one per batch)
+  forms.plain  the same batches as 256 separate launches (one per batch)
   e2e          queries/s through the same C-ABI call with host buffers:
                pinned H2D of the queries and D2H of every result pair inside
                the timed region
   roofline     algorithmic bytes per launch / launch time vs measured HBM peak
   cpu_baseline CPU oracle (grid filter + the reference's predicates) on the
                host cores over a bounded sample of the same queries
+  parity       after timing: per-batch pair counts and order-independent pair
+               digests of the last timed launch against the oracle over the
+               same inputs, at full size (a mismatch exits non-zero)
   clocks       nvidia-smi samples taken during warm-up + timed steps
+  other_configs  (default run, one GPU) reduced runs of configurations 1, 3,
+               4 and 5 with the same keys, each checked against the oracle
+
+Queue capacities are sized exactly by a counting pass before timing (the
+reference's contract: the caller sizes the queue); `sizing_pass` reports
+that pass's own time, which a caller with unknown output sizes pays on top.
 
 --impl reference times the reference's CPU implementation of the path (the
 reference's own predicate code compiled for the host, under the same grid
@@ -62,11 +71,16 @@ def parse():
     ap.add_argument("--sort", type=int, default=-1, help="sort_queries: 0 never, 1 always, 2 auto")
     ap.add_argument("--occupancy", type=int, default=-1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-others", action="store_true",
+                    help="default run only: skip the reduced runs of configs 1, 3, 4, 5")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the full-size comparison with the oracle after timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch settings")
-    ap.add_argument("--rounds", type=int, default=0, help="config 4: mutation rounds (default steps)")
+    ap.add_argument("--rounds", type=int, default=0,
+                    help="config 4: mutation rounds (default 50, the configuration's)")
     ap.add_argument("--requests", type=int, default=600, help="config 5: requests per run")
     return ap.parse_args()
 
@@ -216,6 +230,57 @@ def cpu_query_rate(w, seconds: float, backend: str):
         ora.grid_free(g)
     kindname = "reference" if backend == "ref" else "port"
     return n / best, n, threads, kindname
+
+
+def oracle_backend():
+    """The checker: the reference's own predicate code compiled for the host
+    (oracle/_ref) when that build exists, else the restated oracle."""
+    from oracle.oracle import available
+    return "ref" if available("ref") else "port"
+
+
+KINDS = {"point": 0, "contains": 1, "intersects": 2}
+
+
+def gpu_batch_digests(pairs_h: np.ndarray, counts: np.ndarray, offsets: np.ndarray) -> np.ndarray:
+    """Per-batch order-independent digests of GPU results: batch b's pairs
+    are rows [offsets[b], offsets[b] + counts[b]) of pairs_h."""
+    from oracle.oracle import pair_digest
+    return np.array([pair_digest(pairs_h[int(o):int(o) + int(c)]) if c else 0
+                     for o, c in zip(offsets, counts)], dtype=np.uint64)
+
+
+def oracle_batch_check(w, sizes, gpu_counts: np.ndarray, gpu_digests: np.ndarray,
+                       boxes=None, queries=None) -> dict:
+    """Runs the oracle over the same boxes and queries and compares, batch by
+    batch, the pair count and the order-independent digest of the
+    (geom_id, query_id) pairs, query ids 0-based within each batch as a
+    reference Query call reports them."""
+    from oracle.oracle import Oracle
+    backend = oracle_backend()
+    ora = Oracle(backend)
+    boxes = w["boxes"] if boxes is None else boxes
+    queries = w["queries"] if queries is None else queries
+    sizes = np.asarray(sizes, dtype=np.int64)
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    rid = (np.arange(offs[-1], dtype=np.int64) - np.repeat(offs[:-1], sizes)).astype(np.uint32)
+    t0 = time.perf_counter()
+    total, counts, digests = ora.digest(KINDS[w["kind"]], boxes, queries, rid=rid, grid=True)
+    nz = sizes > 0
+    want_c = np.zeros(len(sizes), dtype=np.uint64)
+    want_d = np.zeros(len(sizes), dtype=np.uint64)
+    if nz.any():
+        want_c[nz] = np.add.reduceat(counts, offs[:-1][nz])
+        want_d[nz] = np.add.reduceat(digests, offs[:-1][nz])
+    bad = np.nonzero((want_c != gpu_counts.astype(np.uint64)) |
+                     (want_d != gpu_digests.astype(np.uint64)))[0]
+    return {"checked": True, "oracle": "reference" if backend == "ref" else "port",
+            "pairs": int(total), "gpu_pairs": int(gpu_counts.sum()), "batches": len(sizes),
+            "equal": bool(bad.size == 0 and int(gpu_counts.sum()) == total),
+            "mismatched_batches": [int(b) for b in bad[:8]],
+            "oracle_seconds": time.perf_counter() - t0,
+            "what": "per-batch pair counts and order-independent (geom_id, query_id) digests "
+                    "vs the oracle on the same inputs"}
 
 
 def run_reference_arm(args, rank: int, world: int):
@@ -411,10 +476,47 @@ def run_query_bench(args, ctx):
     t_main = timed(step_graph, args.steps)
     clocks_info = clocks.stop()
 
+    # Parity at full size, outside every timed region: the last timed launch's
+    # per-batch counts and pair digests against the oracle (rank 0's queries).
+    parity = None
+    if ctx.rank == 0 and not args.no_parity:
+        torch.cuda.synchronize()
+        got_c = qsize.cpu().numpy().astype(np.int64) & 0xFFFFFFFF
+        pairs_h = pairs.cpu().numpy().view(np.uint32)
+        got_d = gpu_batch_digests(pairs_h, np.minimum(got_c, np.maximum(per_batch, 1)),
+                                  poffs[:-1])
+        parity = oracle_batch_check(w, sizes, got_c, got_d)
+        del pairs_h
+
     forms = {}
     if not args.no_plain:
-        for name, fn, k in (("batched_no_graph", step_nograph, max(3, args.steps // 2)),
-                            ("plain", step_plain, max(3, args.steps // 4))):
+        # The counting pass that sized the queues, as a prepared launch: what a
+        # caller that does not know its output sizes pays before each step.
+        count_batches = [(pred, qslices[i], rb.Handler.COUNT, counters[i:i + 1].data_ptr())
+                         for i in range(nbatch)]
+        count_plan = ix.plan(count_batches)
+
+        def step_count():
+            counters.zero_()
+            count_plan.launch(graph=True)
+
+        step_count()
+        torch.cuda.synchronize()
+        if not np.array_equal(counters.cpu().numpy().astype(np.int64), per_batch):
+            raise SystemExit("counting launch differs from the sizing pass")
+        t = timed(step_count, max(3, args.steps // 2))
+        ms = ctx.max(sum(t) / len(t))
+        forms["sizing_pass"] = {
+            "ms_per_step": ms, "launches_per_step": 1,
+            "two_pass_value": nq * ctx.world / ((ms + ctx.max(sum(t_main) / len(t_main))) / 1000),
+            "unit": "queries/s",
+            "what": "counting launch of the same batches (prepared, graph); two_pass_value = "
+                    "queries/s of count-then-collect for callers that size queues per step"}
+        count_plan.close()
+        form_list = [("batched_no_graph", step_nograph, max(3, args.steps // 2))]
+        if nbatch > 1:  # one batch: the plain form is the launch without a graph
+            form_list.append(("plain", step_plain, max(3, args.steps // 4)))
+        for name, fn, k in form_list:
             fn()
             if checksum() != cs:
                 raise SystemExit(f"{name} results differ from the graph launch")
@@ -518,6 +620,7 @@ def run_query_bench(args, ctx):
                "sample": f"first {n} of {nq} queries against all {w['boxes'].shape[0]} boxes, "
                          f"uniform-grid filter, OpenMP, counting only, best of 3"}
 
+    line = None
     if ctx.rank == 0:
         line = {
             "metric": METRIC,
@@ -557,11 +660,14 @@ def run_query_bench(args, ctx):
                          "algorithmic_bytes_per_launch": alg,
                          "kernel": "rts::k_query (+ order sort when enabled)"},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clocks_info,
             "gpu_launches": args.steps * kernels_per_step(ix.config, nq, nbatch, int(pred)),
         }
-        print(json.dumps(line), flush=True)
     plan.close()
+    if parity is not None and not parity["equal"]:
+        raise SystemExit(f"parity check failed: {parity}")
+    return line if ctx.rank == 0 else None
 
 
 def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1) -> int:
@@ -594,10 +700,20 @@ def kernels_per_step(cfg, nq: int, nbatch: int, pred: int = 1, handler: int = 1)
 
 def run_mutable_bench(args, ctx):
     """Config 4: 20M boxes; each round deletes 1%, inserts 1%, updates 2%
-    (moved by U[-1e-3, 1e-3]) and answers 1M point queries.  One step = one
-    round, mutations included; the refit-vs-rebuild threshold is tuned online
-    from the measured round query times.  Every 10th round the counts are
-    checked against a freshly built index of the same boxes."""
+    (moved by U[-1e-3, 1e-3]) and answers 1M point queries (counting
+    handler).  One step = one round, mutations included; the refit-vs-rebuild
+    threshold is tuned online from the measured round query times.
+
+    Every round (warm-up rounds included) is checked against the oracle,
+    outside the timed region: the same points run once more with the
+    collecting handler, and the pair count and order-independent pair digest
+    are compared with the oracle's over a host copy of the box set that
+    applies the reference's semantics (Delete = Envelope::Invalid, Update =
+    overwrite, Insert = append).
+
+    e2e: the same round through the public API with host buffers: pinned H2D
+    of the round's deletes, inserts, updates and points, the round, and D2H of
+    the count, timed on the device per round."""
     torch = ctx.torch
     import rtspatial_b200 as rb
     from rtspatial_b200 import workloads as wl
@@ -609,81 +725,167 @@ def run_mutable_bench(args, ctx):
     ix = make_index(args, rb)
     ix.Insert(torch.from_numpy(state).to(dev))
     torch.cuda.synchronize()
-    rounds = args.rounds or args.steps
+    rounds = args.rounds or 50
     stream = torch.cuda.current_stream()
     counter = torch.zeros(1, dtype=torch.int64, device=dev)
+    count_h = torch.zeros(1, dtype=torch.int64).pin_memory()
     rows, checks = [], []
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     n_live = n0
     clocks = ClockSampler(ctx.local)
     clocks.start()
-    total_ms = 0.0
+    total_ms = e2e_ms = 0.0
+    h2d_bytes = 0
+    check = ctx.rank == 0 and not args.no_parity
+    w_chk = {"kind": "point"}
     for r in range(args.warmup + rounds):
         del_ids, ins, upd_ids, upd, pts = wl.config4_round(rng, n_live, state.shape[0], nq,
                                                             current=state)
-        d_del = torch.from_numpy(del_ids).to(dev)
-        d_ins = torch.from_numpy(ins).to(dev)
-        d_uid = torch.from_numpy(upd_ids).to(dev)
-        d_upd = torch.from_numpy(upd).to(dev)
-        d_pts = torch.from_numpy(pts).to(dev)
+        host = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+                for a in (del_ids, ins, upd_ids, upd, pts)]
         flush.fill_(1.0)
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ctx.barrier()
         torch.cuda.synchronize()
         e[0].record(stream)
+        d_del, d_ins, d_uid, d_upd, d_pts = (h.to(dev, non_blocking=True) for h in host)
+        e[1].record(stream)
         ix.Delete(d_del)
         ix.Update(d_uid, d_upd)
         ix.Insert(d_ins)
-        e[1].record(stream)
+        e[2].record(stream)
         counter.zero_()
         ix.Query(rb.Predicate.kContains, d_pts, counter.data_ptr(), handler=rb.Handler.COUNT)
-        e[2].record(stream)
+        e[3].record(stream)
+        count_h.copy_(counter, non_blocking=True)
+        e[4].record(stream)
         torch.cuda.synchronize()
-        maint_ms, query_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+        maint_ms, query_ms = e[1].elapsed_time(e[2]), e[2].elapsed_time(e[3])
+        round_e2e_ms = e[0].elapsed_time(e[4])
         thr = ix.report_query_time(query_ms)
         state[del_ids, 2] = state[del_ids, 0]
         state[del_ids, 3] = state[del_ids, 1]
         state[upd_ids] = upd
         state = np.concatenate([state, ins])
         n_live += ins.shape[0] - del_ids.shape[0]
-        got = int(counter.item())
+        got = int(count_h.item())
         if r >= args.warmup:
             total_ms += maint_ms + query_ms
+            e2e_ms += round_e2e_ms
+            h2d_bytes = sum(int(h.numel() * h.element_size()) for h in host)
             rows.append({"round": r - args.warmup, "maintenance_ms": maint_ms,
-                         "query_ms": query_ms, "pairs": got, "trees": ix.num_trees(),
-                         "rebuild_update_fraction": thr})
-        if r % 10 == 9 or r == args.warmup + rounds - 1:
-            fresh = rb.SpatialIndex(rb.Config(node_width=ix.config.node_width))
-            fresh.Insert(torch.from_numpy(state).to(dev))
-            c2 = torch.zeros(1, dtype=torch.int64, device=dev)
-            fresh.Query(rb.Predicate.kContains, d_pts, c2.data_ptr(), handler=rb.Handler.COUNT)
+                         "query_ms": query_ms, "e2e_ms": round_e2e_ms, "pairs": got,
+                         "trees": ix.num_trees(), "rebuild_update_fraction": thr})
+        if check:
+            qu = rb.Queue(max(got, 1), dev)
+            ix.Query(rb.Predicate.kContains, d_pts, qu.DeviceObject(), handler=rb.Handler.COLLECT)
             torch.cuda.synchronize()
-            checks.append(int(c2.item()) == got)
-            if not checks[-1]:
-                raise SystemExit(f"round {r}: mutated index {got} pairs, fresh index {int(c2.item())}")
-            del fresh
+            n_col = qu.size()
+            pairs_h = qu.pairs[:min(n_col, max(got, 1))].cpu().numpy().view(np.uint32)
+            got_d = gpu_batch_digests(pairs_h, np.array([min(n_col, max(got, 1))]),
+                                      np.array([0]))
+            res = oracle_batch_check(w_chk, [nq], np.array([n_col], dtype=np.int64), got_d,
+                                     boxes=state, queries=pts)
+            res["count_handler_equal"] = got == res["pairs"]
+            checks.append(res)
+            if not (res["equal"] and res["count_handler_equal"]):
+                raise SystemExit(f"round {r}: mutated index differs from the oracle: {res}")
+            del qu, pairs_h
     clocks_info = clocks.stop()
     step_ms = ctx.max(total_ms / rounds)
-    if ctx.rank == 0:
-        q = np.array([x["query_ms"] for x in rows])
-        m = np.array([x["maintenance_ms"] for x in rows])
-        print(json.dumps({
-            "metric": METRIC, "value": nq * ctx.world / (step_ms / 1000), "unit": "queries/s",
-            "n_gpus": ctx.world, "steps": rounds, "warmup": args.warmup, "ms_per_step": step_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded numpy generators with the configuration's shapes)",
-            "config": {"workload": f"mutable index: {n0} boxes (sides U[0,1e-3]); per round 1% "
-                                   f"deletes, 1% inserts, 2% updates (moved U[-1e-3,1e-3]), "
-                                   f"{nq} uniform point queries; step = one round",
-                       "node_width": ix.config.node_width},
-            "rounds": {"query_ms_p50": float(np.median(q)), "query_ms_max": float(q.max()),
-                       "maintenance_ms_p50": float(np.median(m)),
-                       "maintenance_ms_max": float(m.max()),
-                       "final_rebuild_update_fraction": rows[-1]["rebuild_update_fraction"],
-                       "trees_max": max(x["trees"] for x in rows)},
-            "checks_vs_fresh_index": {"rounds_checked": len(checks), "all_equal": all(checks)},
-            "clocks": clocks_info,
-        }), flush=True)
+    e2e_step_ms = ctx.max(e2e_ms / rounds)
+    if ctx.rank != 0:
+        return None
+    q = np.array([x["query_ms"] for x in rows])
+    m = np.array([x["maintenance_ms"] for x in rows])
+    pairs_med = int(np.median([x["pairs"] for x in rows]))
+    n_final = int(state.shape[0])
+    alg = 16 * n_final + 8 * nq + 8 * pairs_med
+    achieved = alg / (float(np.median(q)) / 1000) / 1e9
+    peak, peak_src = peak_hbm()
+    cpu = None
+    if ctx.world == 1 and not args.no_cpu:
+        rate, n, cores, kind = cpu_query_rate({"kind": "point", "boxes": state, "queries": pts},
+                                              args.cpu_seconds, "ref")
+        cpu = {"value": rate, "unit": "queries/s", "cores": cores, "kind": kind,
+               "sample": f"first {n} of the last round's {nq} points against its {n_final} boxes, "
+                         f"uniform-grid filter (built outside the timing), OpenMP, counting only, "
+                         f"best of 3; queries only, no index maintenance"}
+    return {
+        "metric": METRIC, "value": nq * ctx.world / (step_ms / 1000), "unit": "queries/s",
+        "n_gpus": ctx.world, "steps": rounds, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy generators with the configuration's shapes)",
+        "config": {"workload": f"mutable index: {n0} boxes (sides U[0,1e-3]); per round 1% "
+                               f"deletes, 1% inserts, 2% updates (moved U[-1e-3,1e-3]), "
+                               f"{nq} uniform point queries (counting handler); step = one "
+                               f"round, mutations included",
+                   "node_width": ix.config.node_width, "rounds": rounds,
+                   "l2": "index > L2 and L2 flushed before every round (256 MiB write "
+                         "outside the events)"},
+        "rounds": {"query_ms_p50": float(np.median(q)), "query_ms_max": float(q.max()),
+                   "maintenance_ms_p50": float(np.median(m)),
+                   "maintenance_ms_max": float(m.max()),
+                   "final_rebuild_update_fraction": rows[-1]["rebuild_update_fraction"],
+                   "trees_max": max(x["trees"] for x in rows)},
+        "latency_ms": {"p50": float(np.percentile(q + m, 50)),
+                       "p99": float(np.percentile(q + m, 99)),
+                       "what": "one round (maintenance + query), device time"},
+        "e2e": {"value": nq * ctx.world / (e2e_step_ms / 1000), "unit": "queries/s",
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": 8,
+                "ms_per_step": e2e_step_ms,
+                "path": "per round: pinned H2D of deletes, inserts, updates and points, "
+                        "Delete/Update/Insert/Query(count) through the public API, D2H of the "
+                        "count; device events around all of it"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": alg,
+                     "kernel": "rts::k_query point-contains (median round query time)"},
+        "cpu_baseline": cpu,
+        "parity": {"checked": bool(checks), "oracle": checks[-1]["oracle"] if checks else None,
+                   "rounds_checked": len(checks),
+                   "equal": all(c["equal"] and c["count_handler_equal"] for c in checks),
+                   "pairs_last_round": checks[-1]["pairs"] if checks else None,
+                   "what": "every round (warm-up included): count-handler total, and the "
+                           "collected pairs' count and order-independent digest, vs the oracle "
+                           "over the host mirror of the mutated box set"},
+        "clocks": clocks_info,
+    }
+
+
+def serving_check(sv, reqs, boxes, out_buf, grid=None) -> dict:
+    """Submits `reqs` (closed loop), takes every request's pairs and compares
+    each request's count and order-independent pair digest with the oracle
+    over `boxes` (query ids 0-based per request)."""
+    from oracle.oracle import KIND_CONTAINS, KIND_INTERSECTS, KIND_POINT, Oracle, pair_digest
+    import rtspatial_b200 as rb
+    backend = oracle_backend()
+    ora = Oracle(backend)
+    tickets = [sv.submit(p, q) for p, q in reqs]
+    got = []
+    for t in tickets:
+        pr = sv.take(t, out=out_buf)
+        got.append((int(pr.shape[0]), pair_digest(pr)))
+    t0 = time.perf_counter()
+    own = grid is None
+    g = ora.grid_build(boxes, 2.0) if own else grid
+    bad, total = [], 0
+    try:
+        for i, ((p, q), (n, d)) in enumerate(zip(reqs, got)):
+            if q.shape[1] == 2:
+                kind = KIND_POINT
+            else:
+                kind = KIND_INTERSECTS if p == rb.Predicate.kIntersects else KIND_CONTAINS
+            tot, _c, dig = ora.digest(kind, boxes, q, grid=g)
+            total += tot
+            if tot != n or int(dig.sum(dtype=np.uint64)) != d:
+                bad.append(i)
+    finally:
+        if own:
+            ora.grid_free(g)
+    return {"requests": len(reqs), "pairs": total, "equal": not bad,
+            "mismatched_requests": bad[:8], "oracle": "reference" if backend == "ref" else "port",
+            "oracle_seconds": time.perf_counter() - t0}
 
 
 def run_serving_bench(args, ctx):
@@ -692,7 +894,13 @@ def run_serving_bench(args, ctx):
     arrive as a Poisson stream at 70% of the closed-loop capacity measured
     first, with update batches of 0.1% of the boxes interleaved (one per ten
     requests).  Reports p50/p99 request latency (submit -> pairs on the host)
-    and the served queries/s."""
+    and the served queries/s.
+
+    Parity (rank 0, untimed): every closed-loop request is compared with the
+    oracle on the initial box set (the closed loop runs before any update),
+    and a closed tail of requests submitted after the open loop is compared
+    with the oracle on the final box set, mirrored on the host with the
+    reference's semantics (deletes, then updates, then inserts per batch)."""
     torch = ctx.torch
     import rtspatial_b200 as rb
     from rtspatial_b200 import workloads as wl
@@ -704,6 +912,7 @@ def run_serving_bench(args, ctx):
     torch.cuda.synchronize()
     rng = np.random.default_rng(7 + ctx.rank)
     n_req = args.requests
+    check = ctx.rank == 0 and not args.no_parity
 
     def make_requests(k):
         out = []
@@ -718,12 +927,16 @@ def run_serving_bench(args, ctx):
                 out.append((rb.Predicate.kIntersects, wl.uniform_boxes(rng, n, 1e-3)))
         return out
 
+    n_ids = [nb]
+
     def make_update():
         k = max(1, int(nb * 0.001) // 3)
-        ids = rng.choice(nb, 2 * k, replace=False)
-        return dict(delete_ids=ids[:k], update_ids=ids[k:],
-                    update_boxes=wl.uniform_boxes(rng, k, 1e-3),
-                    inserts=wl.uniform_boxes(rng, k, 1e-3))
+        ids = rng.choice(n_ids[0], 2 * k, replace=False)
+        u = dict(delete_ids=ids[:k], update_ids=ids[k:],
+                 update_boxes=wl.uniform_boxes(rng, k, 1e-3),
+                 inserts=wl.uniform_boxes(rng, k, 1e-3))
+        n_ids[0] += k
+        return u
 
     sv = rb.Server(ix, slots=3, max_queries_per_launch=1 << 19, pairs_per_launch=16 << 20,
                    host_result_bytes=4 << 30)
@@ -747,12 +960,16 @@ def run_serving_bench(args, ctx):
     closed = sv.stats()
     total_q = sum(q.shape[0] for _, q in reqs)
     capacity_qps = total_q / closed_s
+    parity = {}
+    if check:
+        parity["initial"] = serving_check(sv, reqs, boxes, out_buf)
     # open loop: Poisson arrivals at 70% of capacity, updates interleaved
     mean_q = total_q / n_req
     lam = 0.7 * capacity_qps / mean_q
     reqs = make_requests(n_req)
     gaps = rng.exponential(1.0 / lam, n_req)
     ups = [make_update() for _ in range(n_req // 10)]
+    applied = []
     sv.reset_stats()
     clocks = ClockSampler(ctx.local)
     clocks.start()
@@ -768,7 +985,9 @@ def run_serving_bench(args, ctx):
             time.sleep(min(d, 0.002))
         tickets.append(sv.submit(p, q))
         if i % 10 == 9 and ups:
-            up_tickets.append(sv.submit_update(**ups.pop()))
+            u = ups.pop(0)
+            applied.append(u)
+            up_tickets.append(sv.submit_update(**u))
     for t in tickets:
         take(t)
     for t in up_tickets:
@@ -776,31 +995,48 @@ def run_serving_bench(args, ctx):
     open_s = time.perf_counter() - t0
     clocks_info = clocks.stop()
     st = sv.stats()
+    if check:
+        # the host mirror of the box set after every applied update batch
+        final = boxes
+        for u in applied:
+            final[u["delete_ids"], 2] = final[u["delete_ids"], 0]
+            final[u["delete_ids"], 3] = final[u["delete_ids"], 1]
+            final[u["update_ids"]] = u["update_boxes"]
+            final = np.concatenate([final, u["inserts"]])
+        parity["final"] = serving_check(sv, make_requests(max(10, n_req // 20)), final, out_buf)
     sv.close()
     served_q = sum(q.shape[0] for _, q in reqs)
-    if ctx.rank == 0:
-        print(json.dumps({
-            "metric": METRIC, "value": served_q * ctx.world / open_s, "unit": "queries/s",
-            "n_gpus": ctx.world, "steps": n_req, "warmup": 20, "ms_per_step": 1000 * open_s / n_req,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded numpy generators with the configuration's shapes)",
-            "config": {"workload": f"serving: {nb} resident boxes (half uniform, half 64-cluster); "
-                                   f"{n_req} requests, sizes log-uniform [1,100K], 50% point / "
-                                   f"25% contains / 25% intersects, Poisson arrivals at 70% of "
-                                   f"closed-loop capacity, update batches of 0.1% every 10 requests",
-                       "slots": 3},
-            "latency_ms": {"p50": 1000 * st["latency_p50_s"], "p99": 1000 * st["latency_p99_s"],
-                           "max": 1000 * st["latency_max_s"],
-                           "what": "request submit -> its pairs on the host"},
-            "closed_loop": {"queries_per_s": capacity_qps,
-                            "p50_ms": 1000 * closed["latency_p50_s"],
-                            "p99_ms": 1000 * closed["latency_p99_s"],
-                            "launches": closed["launches"]},
-            "open_loop": {"offered_requests_per_s": lam, "launches": st["launches"],
-                          "pairs": st["pairs_done"], "retried_parts": st["retried_parts"],
-                          "updates": st["updates_done"]},
-            "clocks": clocks_info,
-        }), flush=True)
+    if parity and not all(v["equal"] for v in parity.values()):
+        raise SystemExit(f"served results differ from the oracle: {parity}")
+    if ctx.rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": served_q * ctx.world / open_s, "unit": "queries/s",
+        "n_gpus": ctx.world, "steps": n_req, "warmup": 20, "ms_per_step": 1000 * open_s / n_req,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy generators with the configuration's shapes)",
+        "config": {"workload": f"serving: {nb} resident boxes (half uniform, half 64-cluster); "
+                               f"{n_req} requests, sizes log-uniform [1,100K], 50% point / "
+                               f"25% contains / 25% intersects, Poisson arrivals at 70% of "
+                               f"closed-loop capacity, update batches of 0.1% every 10 requests",
+                   "slots": 3},
+        "latency_ms": {"p50": 1000 * st["latency_p50_s"], "p99": 1000 * st["latency_p99_s"],
+                       "max": 1000 * st["latency_max_s"],
+                       "what": "request submit -> its pairs on the host"},
+        "closed_loop": {"queries_per_s": capacity_qps,
+                        "p50_ms": 1000 * closed["latency_p50_s"],
+                        "p99_ms": 1000 * closed["latency_p99_s"],
+                        "launches": closed["launches"]},
+        "open_loop": {"offered_requests_per_s": lam, "launches": st["launches"],
+                      "pairs": st["pairs_done"], "retried_parts": st["retried_parts"],
+                      "updates": st["updates_done"]},
+        "parity": {"checked": bool(parity), "equal": all(v["equal"] for v in parity.values()),
+                   **parity,
+                   "what": "every closed-loop request vs the oracle on the initial boxes; a "
+                           "closed tail after the open loop vs the oracle on the final boxes "
+                           "(per request: pair count and order-independent digest)"},
+        "clocks": clocks_info,
+    }
 
 
 def main():
@@ -811,14 +1047,48 @@ def main():
         return
     ctx = Ctx()
     try:
-        if args.config in (1, 2, 3):
-            run_query_bench(args, ctx)
-        elif args.config == 4:
-            run_mutable_bench(args, ctx)
-        else:
-            run_serving_bench(args, ctx)
+        line = run_config(args, ctx)
+        if args.config == 2 and ctx.world == 1 and not args.no_others:
+            line["other_configs"] = run_other_configs(args, ctx)
+        if ctx.rank == 0:
+            print(json.dumps(line), flush=True)
     finally:
         ctx.close()
+
+
+def run_config(args, ctx):
+    if args.config in (1, 2, 3):
+        return run_query_bench(args, ctx)
+    if args.config == 4:
+        return run_mutable_bench(args, ctx)
+    return run_serving_bench(args, ctx)
+
+
+# Reduced runs of the other configurations that the default (config 2) run
+# nests in its line: full-size inputs, fewer steps.
+OTHER_CONFIGS = {1: dict(steps=10), 3: dict(steps=10), 4: dict(rounds=4, warmup=1),
+                 5: dict(requests=200)}
+
+
+def run_other_configs(args, ctx) -> dict:
+    import copy
+    out = {}
+    for cfg, over in OTHER_CONFIGS.items():
+        a = copy.copy(args)
+        a.config = cfg
+        a.warmup = min(args.warmup, 3)
+        a.cpu_seconds = min(args.cpu_seconds, 6.0)
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.perf_counter()
+        line = run_config(a, ctx)
+        ctx.torch.cuda.empty_cache()
+        keep = ("value", "unit", "ms_per_step", "steps", "warmup", "config", "latency_ms",
+                "pairs_per_s", "pairs_per_step", "forms", "e2e", "roofline", "cpu_baseline",
+                "parity", "rounds", "closed_loop", "open_loop", "autotune", "clocks")
+        out[f"config{cfg}"] = {k: line[k] for k in keep if k in line}
+        out[f"config{cfg}"]["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 if __name__ == "__main__":

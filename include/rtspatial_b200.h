@@ -139,6 +139,9 @@ typedef struct rts_config {
                                     predicate and handler; others run depth-first) */
 #define RTS_TRAVERSAL_PACKET 4 /* one warp walks a packet of up to 32 queries, one entry
                                   per lane; best with sorted queries */
+#define RTS_TRAVERSAL_STAGED 5 /* one thread per query; each visited node group (and a
+                                  leaf group's ids) is bulk-copied into shared memory
+                                  (node_width <= 16; wider indexes use THREAD) */
 
 #define RTS_CURVE_MORTON 0
 #define RTS_CURVE_HILBERT 1
@@ -331,18 +334,23 @@ int rts_server_take(rts_server* server, uint64_t ticket, rts_pair* out, uint64_t
 int rts_server_get_stats(rts_server* server, rts_server_stats* stats);
 int rts_server_reset_stats(rts_server* server);
 
-/* No counterpart in the reference.  The same as rts_query_batched, but it
- * allocates no memory: for callers that cannot call cudaMalloc once they are
- * serving (HBM reserved up front, allocation forbidden on the request path,
- * buffers only from the host engine's own memory manager).  Its scratch — the
- * device work counter and the device copy of the batch descriptors — is a
- * fixed array in the library (about 49 KB per device that loads it, held until
- * the process exits) instead of index-owned buffers.  At most
+/* No counterpart in the reference.  The same arguments, checks and results
+ * as rts_query_batched (float and _F64 query kinds, the same traversal
+ * scheme), but it allocates no memory: for callers that cannot call
+ * cudaMalloc once they are serving (HBM reserved up front, allocation
+ * forbidden on the request path, buffers only from the host engine's own
+ * memory manager).  Its scratch — the device work counter and the device copy
+ * of the batch descriptors — is a fixed array in the library (about 49 KB per
+ * device that loads it, held until the process exits) instead of index-owned
+ * buffers.  Queries are visited in the order given: the curve-order sort of
+ * rts_query_batched needs scratch the size of the launch, so this call skips
+ * it (same pairs, possibly slower on large unsorted batches).  At most
  * RTS_NOALLOC_MAX_BATCHES non-empty batches per call (RTS_ERR_CAPACITY
- * otherwise).  All calls on a device share that array: calls that overlap on
- * the GPU race.  The first call on a device looks up the array's device
- * address; make it before any stream capture.  The index must already be
- * built; inputs and outputs are the caller's, as in rts_query_batched. */
+ * otherwise; empty batches do not count).  All calls on a device share that
+ * array: calls that overlap on the GPU race.  The first call on a device looks
+ * up the array's device address; make it before any stream capture.  The
+ * index must already be built; inputs and outputs are the caller's, as in
+ * rts_query_batched. */
 #define RTS_NOALLOC_MAX_BATCHES 1024
 int rts_query_batched_noalloc(rts_index* index, const rts_batch* batches, uint32_t n_batches,
                               void* stream);
@@ -353,6 +361,13 @@ uint32_t rts_num_trees(const rts_index* index);  /* sub-trees currently indexed 
 /* Device bytes held by the index (SpatialIndex::PrintMemoryUsage,
  * spatial_index.cuh:893-903). */
 uint64_t rts_memory_usage(const rts_index* index);
+/* No counterpart in the reference.  Waits for `stream` and reads the index's
+ * device status word: bits that query kernels set when they stopped early
+ * instead of spinning on (bit 0: a bounded wait for a shared-memory bulk copy
+ * of the staged scheme ran out; the launch's results are then incomplete).
+ * 0 after every launch that completed normally.  The bits stay set. */
+#define RTS_STATUS_WAIT_TIMEOUT 1u
+int rts_device_status(rts_index* index, uint32_t* status, void* stream);
 /* Message of the last failing call on this thread ("" if none). */
 const char* rts_last_error(void);
 /* Library version string. */

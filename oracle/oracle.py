@@ -52,12 +52,43 @@ def _bind(lib: ctypes.CDLL, pfx: str) -> None:
     f = getattr(lib, pfx + "run")
     f.restype = _u64
     f.argtypes = [_vp, _vp, _u64, ctypes.c_int, _vp, _u64, _vp, _vp, _u64, ctypes.c_int]
+    f = getattr(lib, pfx + "run_digest")
+    f.restype = _u64
+    f.argtypes = [_vp, _vp, _u64, ctypes.c_int, _vp, _u64, _vp, _vp, _vp, ctypes.c_int]
     f = getattr(lib, pfx + "eval_pairs")
     f.restype = None
     f.argtypes = [ctypes.c_int, _vp, _vp, _u64, _vp]
     f = getattr(lib, pfx + "invalidate")
     f.restype = None
     f.argtypes = [_vp, _vp, _u64]
+
+
+def pair_mix(geom_ids: np.ndarray, query_ids: np.ndarray) -> np.ndarray:
+    """Digest term of each (geom_id, query_id) pair, as ``ob_pair_mix`` in
+    grid_driver.h computes it (splitmix64's finaliser of geom << 32 | query),
+    in uint64 arithmetic modulo 2^64."""
+    x = (np.asarray(geom_ids).astype(np.uint64) << np.uint64(32)) | \
+        np.asarray(query_ids).astype(np.uint64)
+    x ^= x >> np.uint64(30)
+    x *= np.uint64(0xbf58476d1ce4e5b9)
+    x ^= x >> np.uint64(27)
+    x *= np.uint64(0x94d049bb133111eb)
+    x ^= x >> np.uint64(31)
+    return x
+
+
+def pair_digest(pairs: np.ndarray) -> int:
+    """Order-independent digest of an (R, 2) array of (geom_id, query_id):
+    the sum modulo 2^64 of ``pair_mix`` over its rows."""
+    pairs = np.asarray(pairs).reshape(-1, 2)
+    if pairs.shape[0] == 0:
+        return 0
+    total = np.uint64(0)
+    step = 1 << 24  # bounded temporaries for large result sets
+    for i in range(0, pairs.shape[0], step):
+        part = pairs[i:i + step]
+        total += pair_mix(part[:, 0], part[:, 1]).sum(dtype=np.uint64)
+    return int(total)
 
 
 def _bind64(lib: ctypes.CDLL, pfx: str) -> None:
@@ -148,6 +179,33 @@ class Oracle:
 
     def grid_free(self, g: int) -> None:
         self._f("grid_free")(g)
+
+    def digest(self, kind: int, boxes: np.ndarray, queries: np.ndarray, *,
+               rid: np.ndarray | None = None, grid=None, threads: int | None = None,
+               boxes_per_cell: float = 2.0):
+        """Returns (total, per-query counts, per-query digests): query q's
+        digest is the sum modulo 2^64 of pair_mix(geom_id, rid[q]) over its
+        matches (rid None: rid[q] = q).  ``grid``: a prebuilt grid handle,
+        True (build one here), or False (brute force)."""
+        boxes = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 4)
+        width = 2 if kind == KIND_POINT else 4
+        queries = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, width)
+        nb, nq = boxes.shape[0], queries.shape[0]
+        if rid is not None:
+            rid = np.ascontiguousarray(rid, dtype=np.uint32)
+            assert rid.shape[0] == nq
+        threads = threads or os.cpu_count() or 1
+        own = grid is None or grid is True
+        g = self._f("grid_build")(_ptr(boxes), nb, boxes_per_cell) if own else (grid or None)
+        try:
+            counts = np.zeros(max(nq, 1), dtype=np.uint64)
+            digests = np.zeros(max(nq, 1), dtype=np.uint64)
+            total = int(self._f("run_digest")(g, _ptr(boxes), nb, kind, _ptr(queries), nq,
+                                              _ptr(rid), _ptr(counts), _ptr(digests), threads))
+            return total, counts[:nq], digests[:nq]
+        finally:
+            if own and g:
+                self._f("grid_free")(g)
 
     def run_on_grid(self, g: int, kind: int, boxes: np.ndarray, queries: np.ndarray,
                     threads: int) -> int:

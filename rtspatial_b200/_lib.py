@@ -30,6 +30,8 @@ RTS_TRAVERSAL_THREAD = 1
 RTS_TRAVERSAL_TEAM = 2
 RTS_TRAVERSAL_FRONTIER = 3
 RTS_TRAVERSAL_PACKET = 4
+RTS_TRAVERSAL_STAGED = 5
+RTS_STATUS_WAIT_TIMEOUT = 1
 RTS_CURVE_MORTON = 0
 RTS_CURVE_HILBERT = 1
 RTS_QUERY_POINTS = 0
@@ -136,6 +138,7 @@ SIGNATURES = {
     "rts_query_envelopes_f64": (_I, [_P, _I, _P, _U64, _I, _P, _P]),
     "rts_query_batched": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_query_batched_noalloc": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
+    "rts_device_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _P]),
     "rts_plan_create": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, ctypes.POINTER(_P)]),
     "rts_plan_launch": (_I, [_P, _P, _I]),
     "rts_plan_destroy": (_I, [_P]),

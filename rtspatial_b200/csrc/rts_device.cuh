@@ -62,6 +62,64 @@ __device__ __forceinline__ void ldg_box_pair(const float4* p, float4& a, float4&
                   __uint_as_float(static_cast<uint32_t>(x3 >> 32)));
 }
 
+// ---------------------------------------------------------------------------
+// Bulk copies into shared memory (the staged traversal scheme).  A copy is
+// issued by one thread with cp.async.bulk (the TMA unit moves the bytes from
+// L2 into shared memory without passing through L1 or registers) and
+// completes on an mbarrier whose transaction count it decrements.  No
+// multicast form is used.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t arrivals) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(arrivals) : "memory");
+}
+// Makes barrier initialisations visible to the async proxy.
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Arrives on the barrier and raises its expected transaction bytes.
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory before
+// later async-proxy (bulk copy) writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// bytes (a multiple of 16) from global src (16-byte aligned) to shared dst
+// (16-byte aligned), completing on barrier bar.
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                              uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+// Spin limit of a barrier wait (each try_wait also suspends for a
+// hardware-chosen time): far beyond any copy's latency, so reaching it means
+// the copy engine stopped answering; the kernel then records kErrWaitTimeout
+// and returns instead of spinning on.
+constexpr uint32_t kWaitSpinLimit = 1u << 22;
+constexpr uint32_t kErrWaitTimeout = 1u;
+
 struct TreeDesc {
   const float4* leaves;  // first slot of this tree
   const DBox* leaves64;  // double index: the double envelopes of the same slots
@@ -76,6 +134,7 @@ struct TreeDesc {
 struct Forest {
   TreeDesc tree[kMaxTrees];
   const uint32_t* ids_base;  // leaf_ids of slot 0 (all sub-trees share the array)
+  uint32_t* err;             // device status word of the index (kErr* bits), or nullptr
   uint32_t n_trees;
   uint32_t width;
 };
@@ -527,7 +586,10 @@ constexpr uint32_t kRouteBits = 6;
 constexpr uint32_t kRouteSlots = 1u << kRouteBits;
 constexpr uint32_t kWarpBatWords = kWarpOutCap + 3 * kRouteSlots;
 
-template <bool ROUTED>
+// RESOLVED: the staged entries already hold geom ids (the staged scheme reads
+// them from its shared-memory copy of the leaf group); otherwise leaf slots,
+// turned into ids at the flush.
+template <bool ROUTED, bool RESOLVED = false>
 struct WarpOut {
   DevPair* buf;              // kWarpOutCap entries in shared memory, private to the warp
   uint32_t* bat;             // merged launch: batch index of each entry, then the
@@ -562,7 +624,7 @@ struct WarpOut {
           const uint32_t i = i0 + lane_id() + 32u * r;
           if (i < n) {
             const DevPair e = buf[i];
-            gid[r] = __ldg(ids + e.geom_id);
+            gid[r] = RESOLVED ? e.geom_id : __ldg(ids + e.geom_id);
             qid[r] = e.query_id;
           }
         }
@@ -614,7 +676,9 @@ struct WarpOut {
         const DevPair e = buf[i];
         const DevQueue Q = routes[b];
         const unsigned long long p = atomicAdd(Q.size, 1u);
-        if (p < Q.capacity) Q.data[p] = DevPair{__ldg(ids + e.geom_id), __ldg(ident + e.query_id)};
+        if (p < Q.capacity)
+          Q.data[p] = DevPair{RESOLVED ? e.geom_id : __ldg(ids + e.geom_id),
+                              __ldg(ident + e.query_id)};
         bat[i] = kEmpty;
       }
     }
@@ -629,7 +693,9 @@ struct WarpOut {
       const uint32_t slot = v >> 16;
       const DevQueue Q = routes[keys[slot]];
       const unsigned long long p = static_cast<unsigned long long>(bases[slot]) + (v & 0xffffu);
-      if (p < Q.capacity) Q.data[p] = DevPair{__ldg(ids + e.geom_id), __ldg(ident + e.query_id)};
+      if (p < Q.capacity)
+        Q.data[p] = DevPair{RESOLVED ? e.geom_id : __ldg(ids + e.geom_id),
+                            __ldg(ident + e.query_id)};
     }
   }
 
@@ -678,6 +744,63 @@ struct WarpOut {
     for (int c = 0; c < W; ++c) {  // the set bits, lowest first (predicated, no divergence)
       if ((m >> c) & 1u) {
         buf[k] = DevPair{slot0 + c, qid};
+        if constexpr (ROUTED) bat[k] = rb;
+        ++k;
+      }
+    }
+    n += total;
+  }
+
+  // Staged scheme: like add<W>, with the geom ids of the lane's leaf group in
+  // shared memory (sid[0..W)); the set bits are visited starting at the
+  // lane's own rotation (c + lane) mod W, which spreads the lanes' reads of
+  // sid over the banks.  The pair order within a flush does not matter.
+  template <int W>
+  __device__ __forceinline__ void add_resolved(const DevQueue& qu, uint32_t m,
+                                               const uint32_t* sid, uint32_t qid, uint32_t rb) {
+    static_assert(RESOLVED, "add_resolved stages geom ids");
+    if (!__any_sync(kFull, m != 0)) return;
+    const uint32_t lane = lane_id();
+    const uint32_t cnt = __popc(m);
+    uint32_t total;
+    const uint32_t excl = warp_excl_prefix<(W >= 32 ? 6 : W >= 16 ? 5 : W >= 8 ? 4 : 3)>(cnt, total);
+    if (n + total > kWarpOutCap) flush(qu);
+    if (total > kWarpOutCap) {  // more than a buffer: straight to the queue(s)
+      if constexpr (ROUTED) {
+        if (cnt) {
+          const DevQueue Q = routes[rb];
+          const uint32_t rid = __ldg(ident + qid);
+          const unsigned long long p0 = atomicAdd(Q.size, cnt);
+          unsigned long long p = p0;
+#pragma unroll
+          for (int c = 0; c < W; ++c) {
+            if ((m >> c) & 1u) {
+              if (p < Q.capacity) Q.data[p] = DevPair{sid[c], rid};
+              ++p;
+            }
+          }
+        }
+      } else {
+        uint32_t base = 0;
+        if (lane == 31) base = atomicAdd(qu.size, total);
+        base = __shfl_sync(kFull, base, 31);
+        unsigned long long p = static_cast<unsigned long long>(base) + excl;
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+          if ((m >> c) & 1u) {
+            if (p < qu.capacity) qu.data[p] = DevPair{sid[c], qid};
+            ++p;
+          }
+        }
+      }
+      return;
+    }
+    uint32_t k = n + excl;
+#pragma unroll
+    for (int c = 0; c < W; ++c) {  // predicated, no divergence
+      const uint32_t idx = (static_cast<uint32_t>(c) + lane) & (W - 1);
+      if ((m >> idx) & 1u) {
+        buf[k] = DevPair{sid[idx], qid};
         if constexpr (ROUTED) bat[k] = rb;
         ++k;
       }

@@ -93,7 +93,13 @@ namespace rts {
 
 int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
   uint64_t need = slots + kSlotAlign;
-  int rc = buf_reserve(ix->leaves, need * sizeof(float4), s, true, ix->slot_end * sizeof(float4));
+  int rc;
+  if (!ix->status.ptr) {  // the device status word the query kernels report into
+    if ((rc = buf_reserve(ix->status, sizeof(uint32_t), s, false, 0))) return rc;
+    RTS_CUDA_TRY(cudaMemsetAsync(ix->status.ptr, 0, sizeof(uint32_t), s));
+    ix->forest_dirty = true;
+  }
+  rc = buf_reserve(ix->leaves, need * sizeof(float4), s, true, ix->slot_end * sizeof(float4));
   if (rc) return rc;
   if (is_f64(ix) &&
       (rc = buf_reserve(ix->leaves64, need * sizeof(DBox), s, true, ix->slot_end * sizeof(DBox))))
@@ -311,6 +317,7 @@ int refresh_forest(rts_index* ix) {
   F.n_trees = static_cast<uint32_t>(ix->trees.size());
   F.width = static_cast<uint32_t>(ix->W);
   F.ids_base = ids_of(ix);
+  F.err = static_cast<uint32_t*>(ix->status.ptr);
   for (size_t i = 0; i < ix->trees.size(); ++i) {
     const HostTree& h = ix->trees[i];
     TreeDesc& d = F.tree[i];
@@ -341,9 +348,11 @@ LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total) {
   // Double indexes run the thread or packet scheme only.
   if (is_f64(ix) && (trav == RTS_TRAVERSAL_TEAM || trav == RTS_TRAVERSAL_FRONTIER))
     trav = RTS_TRAVERSAL_THREAD;
+  if (trav == RTS_TRAVERSAL_STAGED && ix->W > 16) trav = RTS_TRAVERSAL_THREAD;
   p.frontier = (trav == RTS_TRAVERSAL_FRONTIER);
   p.team = (trav == RTS_TRAVERSAL_TEAM);
   p.packet = (trav == RTS_TRAVERSAL_PACKET);
+  p.staged = (trav == RTS_TRAVERSAL_STAGED);
   // Work items: the configured chunk, shrunk for small launches so that every
   // resident warp (about 32 per SM) still gets a few chunks.
   uint32_t chunk = ix->cfg.chunk ? ix->cfg.chunk : 128u;
@@ -429,6 +438,50 @@ int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
                             static_cast<uint32_t*>(qs.ck_order.ptr), qs.sort_temp, s);
 }
 
+// Validates one public batch description against the index and, when the
+// batch is not empty, fills its launch descriptor (chunk_begin and qbase from
+// the running totals, which it advances).  *keep = false for an empty batch.
+int batch_desc(const rts_index* ix, const rts_batch& b, const LaunchPlan& plan, uint64_t& chunks,
+               uint64_t& qsum, BatchDesc& d, bool* keep) {
+  *keep = false;
+  int rc;
+  if ((rc = check_handler(b.handler, b.arg))) return rc;
+  int pred;
+  const bool f64 = b.query_kind == RTS_QUERY_POINTS_F64 || b.query_kind == RTS_QUERY_ENVELOPES_F64;
+  if (b.query_kind == RTS_QUERY_POINTS || b.query_kind == RTS_QUERY_POINTS_F64) {
+    if (b.predicate != RTS_PREDICATE_CONTAINS)
+      return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
+    pred = f64 ? kPoint64 : kPoint;
+  } else if (b.query_kind == RTS_QUERY_ENVELOPES || b.query_kind == RTS_QUERY_ENVELOPES_F64) {
+    if (b.predicate == RTS_PREDICATE_CONTAINS) pred = f64 ? kContains64 : kContains;
+    else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = f64 ? kIntersects64 : kIntersects;
+    else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
+  } else {
+    return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
+  }
+  if (f64 != is_f64(ix))
+    return fail(RTS_ERR_INVALID_ARGUMENT, f64 ? "double queries on a float index"
+                                              : "float queries on a double index (use the _F64 kinds)");
+  if (b.n == 0) return RTS_OK;
+  if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
+  if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
+  d = BatchDesc{};
+  d.queries = b.queries;
+  d.arg = b.arg;
+  d.n = static_cast<uint32_t>(b.n);
+  d.pred = pred;
+  d.mode = b.handler;
+  d.chunk_begin = static_cast<uint32_t>(chunks);
+  d.order = nullptr;
+  d.qbase = static_cast<uint32_t>(qsum);
+  qsum += b.n;
+  if (qsum > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a launch");
+  chunks += (b.n + plan.chunk - 1) / plan.chunk;
+  if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
+  *keep = true;
+  return RTS_OK;
+}
+
 // Turns public batch descriptions into launch descriptors (validating them);
 // empty batches are dropped.  chunks = work items of the launch.
 int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
@@ -437,43 +490,11 @@ int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches
   out.reserve(n_batches);
   chunks = 0;
   uint64_t qsum = 0;
-  int rc;
   for (uint32_t i = 0; i < n_batches; ++i) {
-    const rts_batch& b = batches[i];
-    if ((rc = check_handler(b.handler, b.arg))) return rc;
-    int pred;
-    const bool f64 = b.query_kind == RTS_QUERY_POINTS_F64 || b.query_kind == RTS_QUERY_ENVELOPES_F64;
-    if (b.query_kind == RTS_QUERY_POINTS || b.query_kind == RTS_QUERY_POINTS_F64) {
-      if (b.predicate != RTS_PREDICATE_CONTAINS)
-        return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
-      pred = f64 ? kPoint64 : kPoint;
-    } else if (b.query_kind == RTS_QUERY_ENVELOPES || b.query_kind == RTS_QUERY_ENVELOPES_F64) {
-      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = f64 ? kContains64 : kContains;
-      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = f64 ? kIntersects64 : kIntersects;
-      else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
-    } else {
-      return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
-    }
-    if (f64 != is_f64(ix))
-      return fail(RTS_ERR_INVALID_ARGUMENT, f64 ? "double queries on a float index"
-                                                : "float queries on a double index (use the _F64 kinds)");
-    if (b.n == 0) continue;
-    if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
-    if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
-    BatchDesc d{};
-    d.queries = b.queries;
-    d.arg = b.arg;
-    d.n = static_cast<uint32_t>(b.n);
-    d.pred = pred;
-    d.mode = b.handler;
-    d.chunk_begin = static_cast<uint32_t>(chunks);
-    d.order = nullptr;
-    d.qbase = static_cast<uint32_t>(qsum);
-    qsum += b.n;
-    if (qsum > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a launch");
-    chunks += (b.n + plan.chunk - 1) / plan.chunk;
-    if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
-    out.push_back(d);
+    BatchDesc d;
+    bool keep = false;
+    if (int rc = batch_desc(ix, batches[i], plan, chunks, qsum, d, &keep)) return rc;
+    if (keep) out.push_back(d);
   }
   return RTS_OK;
 }
@@ -635,7 +656,7 @@ int rts_create(const rts_config* cfg, rts_index** out) {
   if (cfg) c = *cfg; else rts_config_default(&c);
   if (c.node_width != 4 && c.node_width != 8 && c.node_width != 16 && c.node_width != 32)
     return fail(RTS_ERR_INVALID_ARGUMENT, "node_width must be 4, 8, 16 or 32");
-  if (c.traversal < 0 || c.traversal > RTS_TRAVERSAL_PACKET)
+  if (c.traversal < 0 || c.traversal > RTS_TRAVERSAL_STAGED)
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad traversal");
   if (c.curve != RTS_CURVE_MORTON && c.curve != RTS_CURVE_HILBERT)
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad curve");
@@ -672,7 +693,7 @@ int rts_destroy(rts_index* ix) {
   DevBuf* all[] = {&ix->leaves, &ix->leaf_ids, &ix->pos, &ix->keys_a, &ix->keys_b, &ix->vals_a,
                    &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp, &ix->leaves64,
                    &ix->rounded, &ix->upd_bits, &ix->upd_ids, &ix->upd_boxes,
-                   &ix->upd_boxes64, &ix->upd_count};
+                   &ix->upd_boxes64, &ix->upd_count, &ix->status};
   for (DevBuf* b : all) {
     touched |= b->ptr != nullptr;
     buf_free(*b, s);
@@ -958,6 +979,16 @@ int rts_report_query_time(rts_index* ix, double query_ms, float* rebuild_update_
   return RTS_OK;
 }
 
+int rts_device_status(rts_index* ix, uint32_t* status, void* stream) {
+  if (!ix || !status) return fail(RTS_ERR_INVALID_ARGUMENT, "index or status is null");
+  *status = 0;
+  if (!ix->status.ptr) return RTS_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  RTS_CUDA_TRY(cudaMemcpyAsync(status, ix->status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  RTS_CUDA_TRY(cudaStreamSynchronize(s));
+  return RTS_OK;
+}
+
 uint64_t rts_size(const rts_index* ix) { return ix ? ix->n_ids : 0; }
 
 uint32_t rts_num_trees(const rts_index* ix) {
@@ -1035,45 +1066,25 @@ extern "C" int rts_query_batched_noalloc(rts_index* ix, const rts_batch* batches
   if (!ix) return fail(RTS_ERR_INVALID_ARGUMENT, "index is null");
   if (n_batches == 0) return RTS_OK;
   if (!batches) return fail(RTS_ERR_INVALID_ARGUMENT, "batches is null");
-  if (n_batches > kNoAllocMaxBatches)
-    return fail(RTS_ERR_CAPACITY, "rts_query_batched_noalloc takes at most " +
-                                      std::to_string(kNoAllocMaxBatches) + " batches, got " +
-                                      std::to_string(n_batches));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BatchDesc descs[kNoAllocMaxBatches];
   uint32_t nd = 0;
-  uint64_t chunks = 0;
+  uint64_t chunks = 0, qsum = 0;
   int rc;
-  LaunchPlan plan = plan_for(ix, kContains, sum_queries(batches, n_batches));
+  // The scheme rts_query_batched would pick for these batches; the queries
+  // are visited in the callers' order (no visiting-order sort, which needs
+  // scratch the size of the launch).
+  LaunchPlan plan = plan_for(ix, launch_pred(batches, n_batches), sum_queries(batches, n_batches));
   for (uint32_t i = 0; i < n_batches; ++i) {
-    const rts_batch& b = batches[i];
-    if ((rc = check_handler(b.handler, b.arg))) return rc;
-    int pred;
-    if (b.query_kind == RTS_QUERY_POINTS) {
-      if (b.predicate != RTS_PREDICATE_CONTAINS)
-        return fail(RTS_ERR_INVALID_ARGUMENT, "points support only the contains predicate");
-      pred = kPoint;
-    } else if (b.query_kind == RTS_QUERY_ENVELOPES) {
-      if (b.predicate == RTS_PREDICATE_CONTAINS) pred = kContains;
-      else if (b.predicate == RTS_PREDICATE_INTERSECTS) pred = kIntersects;
-      else return fail(RTS_ERR_INVALID_ARGUMENT, "unknown predicate");
-    } else {
-      return fail(RTS_ERR_INVALID_ARGUMENT, "unknown query kind");
-    }
-    if (b.n == 0) continue;
-    if (!b.queries) return fail(RTS_ERR_INVALID_ARGUMENT, "batch queries is null");
-    if (b.n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in a batch");
-    BatchDesc& d = descs[nd++];
-    d = BatchDesc{};
-    d.queries = b.queries;
-    d.arg = b.arg;
-    d.n = static_cast<uint32_t>(b.n);
-    d.pred = pred;
-    d.mode = b.handler;
-    d.chunk_begin = static_cast<uint32_t>(chunks);
-    d.order = nullptr;
-    chunks += (b.n + plan.chunk - 1) / plan.chunk;
-    if (chunks > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "too many work items in one launch");
+    BatchDesc d;
+    bool keep = false;
+    if ((rc = batch_desc(ix, batches[i], plan, chunks, qsum, d, &keep))) return rc;
+    if (!keep) continue;
+    if (nd == kNoAllocMaxBatches)
+      return fail(RTS_ERR_CAPACITY, "rts_query_batched_noalloc takes at most " +
+                                        std::to_string(kNoAllocMaxBatches) +
+                                        " non-empty batches per call");
+    descs[nd++] = d;
   }
   if (nd == 0 || ix->n_ids == 0) return RTS_OK;
   void* scratch = nullptr;

@@ -91,6 +91,7 @@ struct rts_index {
   uint64_t updated_since_build = 0;
   uint64_t version = 0;         // bumped when buffers or sub-trees change
   rts::DevBuf leaves, leaf_ids, pos;
+  rts::DevBuf status;           // device status word: kErr* bits set by query kernels
   rts::DevBuf leaves64;         // double index: the double envelopes, slot by slot
   rts::DevBuf rounded;          // double index: scratch of an insert's float rounding
   // scratch of the update split: slot bitmaps, moved ids / envelopes, count

@@ -14,7 +14,12 @@ QueryKernel query_kernel_occ2(const LaunchPlan& p, bool routed);
 QueryKernel query_kernel_occ3(const LaunchPlan& p, bool routed);
 QueryKernel query_kernel_occ4(const LaunchPlan& p, bool routed);
 
+// rts_query_staged.cu
+QueryKernel query_kernel_staged(const LaunchPlan& p, bool routed);
+size_t staged_smem_bytes(int width);
+
 static QueryKernel pick_kernel(const LaunchPlan& p, bool routed) {
+  if (p.staged) return query_kernel_staged(p, routed);
   switch (p.min_blocks) {
     case 4: return query_kernel_occ4(p, routed);
     case 3: return query_kernel_occ3(p, routed);
@@ -35,10 +40,15 @@ int device_sm_count() {
   return g_num_sms;
 }
 
-// Dynamic shared memory of the chosen kernel: the packet scheme's per-warp
-// query tables, and the per-warp batch tables of a merged launch.
+// Dynamic shared memory of the chosen kernel: the staged scheme's per-warp
+// group slots, the packet scheme's per-warp query tables, and the per-warp
+// batch tables of a merged launch.
 static size_t dyn_smem_bytes(const LaunchPlan& p, bool merged) {
   size_t per = 0;
+  if (p.staged) {
+    return staged_smem_bytes(p.width) +
+           (merged ? kWarpBatWords * sizeof(uint32_t) * (kQueryThreads / 32) : 0);
+  }
   if (p.packet) {
     switch (p.width) {
       case 4: per = packet_stride<4>(); break;
@@ -95,6 +105,7 @@ int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
   if (total_chunks == 0) return RTS_OK;
   LaunchPlan use = plan;
   if (only) use.packet = false;  // the packet scheme takes no query filter
+  if (use.staged && use.width > 16) use.staged = false;  // slots hold at most 16 boxes
   QueryKernel k = pick_kernel(use, merged != nullptr);
   if (!k) return fail(RTS_ERR_INVALID_ARGUMENT, "unsupported node width / traversal");
   const size_t dyn = dyn_smem_bytes(use, merged != nullptr);

@@ -183,6 +183,97 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
   }
 }
 
+// Staged scheme (run_chunk_staged): per warp, one StageWarp<W> area at the
+// start of the dynamic shared memory, then (merged launch) the warps' batch
+// tables.  Returns false when a copy wait gave up (the kernel then stops).
+template <int W, bool ROUTED>
+__device__ __noinline__ bool dispatch_staged(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                             uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                             const uint32_t* only, const MergedOrder& M,
+                                             StageWarp<W>& S) {
+#define RTS_RUN(P, H) return run_chunk_staged<P, H, W, ROUTED>(F, B, cb, ce, wbuf, wbat, only, M, S)
+  switch (B.pred * 2 + B.mode) {
+    case kPoint * 2 + kCount: RTS_RUN(kPoint, kCount);
+    case kPoint * 2 + kCollect: RTS_RUN(kPoint, kCollect);
+    case kContains * 2 + kCount: RTS_RUN(kContains, kCount);
+    case kContains * 2 + kCollect: RTS_RUN(kContains, kCollect);
+    case kIntersects * 2 + kCount: RTS_RUN(kIntersects, kCount);
+    case kIntersects * 2 + kCollect: RTS_RUN(kIntersects, kCollect);
+    case kPoint64 * 2 + kCount: RTS_RUN(kPoint64, kCount);
+    case kPoint64 * 2 + kCollect: RTS_RUN(kPoint64, kCollect);
+    case kContains64 * 2 + kCount: RTS_RUN(kContains64, kCount);
+    case kContains64 * 2 + kCollect: RTS_RUN(kContains64, kCollect);
+    case kIntersects64 * 2 + kCount: RTS_RUN(kIntersects64, kCount);
+    case kIntersects64 * 2 + kCollect: RTS_RUN(kIntersects64, kCollect);
+    default: return true;
+  }
+#undef RTS_RUN
+}
+
+template <int W>
+constexpr size_t staged_stride() {
+  return (sizeof(StageWarp<W>) + 15) / 16 * 16;
+}
+
+// Resident CTAs per SM the staged kernels' registers are capped for: what
+// their shared memory (one StageWarp<W> per warp) lets fit on an SM.
+template <int W>
+constexpr int staged_min_blocks() {
+  return W >= 16 ? 2 : (W >= 8 ? 3 : 4);
+}
+
+template <int W, bool ROUTED>
+__global__ void __launch_bounds__(kQueryThreads, staged_min_blocks<W>())
+    k_query_staged(const __grid_constant__ Forest F_in, const __grid_constant__ BatchDesc b0,
+                   const BatchDesc* __restrict__ descs, uint32_t nb, uint32_t total_chunks,
+                   uint32_t chunk, uint32_t* __restrict__ work, const uint32_t* __restrict__ only,
+                   const uint32_t* __restrict__ only_any, const __grid_constant__ MergedOrder M,
+                   const uint32_t* __restrict__ chunk_order) {
+  if (only_any && *only_any == 0) return;
+  __shared__ Forest F;
+  __shared__ DevPair wbufs[kQueryThreads / 32][kWarpOutCap];
+  extern __shared__ __align__(16) unsigned char qdyn[];
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&F_in);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&F);
+    for (uint32_t i = threadIdx.x; i < sizeof(Forest) / 4; i += blockDim.x) dst[i] = src[i];
+  }
+  const uint32_t lane = lane_id();
+  const uint32_t wid = threadIdx.x / 32;
+  StageWarp<W>& S = *reinterpret_cast<StageWarp<W>*>(qdyn + wid * staged_stride<W>());
+  if (lane == 0) {
+    mbar_init(smem_u32(&S.bar), 32);
+    S.phase = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  for (;;) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(work, 1u);
+    c = __shfl_sync(kFull, c, 0);
+    if (c >= total_chunks) break;
+    if (chunk_order) c = __ldg(chunk_order + c);  // c < total_chunks: a permutation
+    BatchDesc B;
+    if (nb == 1) {
+      B = b0;
+    } else {
+      uint32_t lo = 0, hi = nb - 1;  // largest b with chunk_begin <= c
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&descs[mid].chunk_begin) <= c) lo = mid; else hi = mid - 1;
+      }
+      B = descs[lo];
+    }
+    const uint32_t cb = (c - B.chunk_begin) * chunk;
+    const uint32_t ce = min(cb + chunk, B.n);
+    uint32_t* wbat = ROUTED ? reinterpret_cast<uint32_t*>(
+                                  qdyn + (kQueryThreads / 32) * staged_stride<W>()) +
+                                  wid * kWarpBatWords
+                            : nullptr;
+    if (!dispatch_staged<W, ROUTED>(F, B, cb, ce, wbufs[wid], wbat, only, M, S)) break;
+  }
+}
+
 using QueryKernel = void (*)(const Forest, const BatchDesc, const BatchDesc*, uint32_t, uint32_t,
                              uint32_t, uint32_t*, const uint32_t*, const uint32_t*,
                              const MergedOrder, const uint32_t*);

@@ -177,6 +177,153 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
 }
 
 // ---------------------------------------------------------------------------
+// staged scheme: the thread scheme with every group moved into shared memory
+// by the copy engine
+// ---------------------------------------------------------------------------
+// Each lane still owns one query and visits one W-group per step, but the
+// group's boxes (and, at a leaf group, its W geom ids) are not loaded into
+// registers: the lane issues cp.async.bulk copies into its own slot of the
+// warp's shared-memory area, all lanes arrive on the warp's mbarrier (the
+// active ones announcing their bytes), and after the wait each lane tests the
+// W boxes from shared memory one at a time.  So the group holds no registers
+// while it is in flight (the thread scheme's W float4 are its register
+// ceiling), the bytes bypass L1, and hits are staged with their geom ids
+// already read, so the output flush issues no id loads.  Reads start at the
+// lane's rotation (c + lane) mod W: a quarter-warp of lanes then reads eight
+// different 16-byte bank groups of their slots.  Results, visiting order and
+// output contract are those of the thread scheme.  Node width W <= 16.
+template <int W>
+struct StageWarp {
+  float4 grp[32][W];     // each lane's current group
+  uint32_t sid[32][W];   // each lane's leaf ids (leaf steps)
+  unsigned long long bar;  // mbarrier: 32 arrivals per phase plus the copies' bytes
+  uint32_t phase;          // parity of the phase the next wait completes
+  uint32_t pad;
+};
+
+template <int PRED, int MODE, int W, bool ROUTED>
+__device__ __forceinline__ bool run_chunk_staged(const Forest& F, const BatchDesc& B,
+                                                 uint32_t cbeg, uint32_t cend, DevPair* wbuf,
+                                                 uint32_t* wbat, const uint32_t* only,
+                                                 const MergedOrder& M, StageWarp<W>& S) {
+  static_assert(W <= 16, "a staged lane slot holds at most 16 boxes");
+  using Ops = QueryOps<PRED>;
+  const uint32_t lane = lane_id();
+  const uint32_t bar = smem_u32(&S.bar);
+  const uint32_t grp_dst = smem_u32(&S.grp[lane][0]);
+  const uint32_t sid_dst = smem_u32(&S.sid[lane][0]);
+  uint32_t phase = S.phase;
+  TravState<PRED, W> s;
+  uint32_t next = cbeg;
+  bool active = false;
+  {
+    uint32_t slot = next + lane;
+    if (slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
+    next = min(cend, next + 32u);
+  }
+  DevQueue qu{};
+  if (MODE == kCollect && !ROUTED) qu = *static_cast<const DevQueue*>(B.arg);
+  WarpOut<ROUTED, true> out(wbuf, wbat, F.ids_base, M);
+  unsigned long long cnt = 0;
+  bool ok = true;
+
+  for (;;) {
+    if (!__any_sync(kFull, active)) {
+      if (next >= cend) break;  // see run_chunk_thread
+      uint32_t slot = next + lane;
+      if (slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
+      next = min(cend, next + 32u);
+      continue;
+    }
+    // Issue this step's copies.  The fence orders the lane's reads of its
+    // slot in the previous step before the copy engine overwrites it.
+    uint32_t first = 0, lim = 0;
+    bool at_leaf = false;
+    fence_proxy_async_smem();
+    if (active) {
+      const TreeDesc& T = F.tree[s.t];
+      first = s.g * W;
+      at_leaf = (s.L == 0);
+      const float4* p = at_leaf ? T.leaves + first : T.nodes + T.level_off[s.L] + first;
+      lim = (at_leaf ? T.n : T.level_cnt[s.L]) - first;
+      mbar_arrive_tx(bar, at_leaf ? W * 20u : W * 16u);
+      bulk_copy_g2s(grp_dst, p, W * 16u, bar);
+      if (at_leaf) bulk_copy_g2s(sid_dst, T.ids + first, W * 4u, bar);
+    } else {
+      mbar_arrive(bar);
+    }
+    {  // bounded wait for the phase: every lane arrived, every byte landed
+      uint32_t spins = 0;
+      bool done = false;
+      while (!(done = mbar_try_wait(bar, phase)) && ++spins < kWaitSpinLimit) {
+      }
+      if (!__all_sync(kFull, done)) {
+        if (lane == 0 && F.err) atomicOr(F.err, kErrWaitTimeout);
+        // give the copies in flight a second bounded wait before leaving
+        spins = 0;
+        while (!mbar_try_wait(bar, phase) && ++spins < kWaitSpinLimit) {
+        }
+        ok = false;
+        break;
+      }
+      phase ^= 1u;
+    }
+    uint32_t leafm = 0;
+    if (active) {
+      const float4* gl = S.grp[lane];
+      uint32_t m = 0;
+#pragma unroll
+      for (int c = 0; c < W; ++c) {
+        const uint32_t idx = (static_cast<uint32_t>(c) + lane) & (W - 1);
+        const float4 e = gl[idx];
+        if (idx < lim && Ops::coarse(e, s.q)) m |= 1u << idx;
+      }
+      if (at_leaf) {
+        if constexpr (Ops::kNeeds64) {  // exact test on the slots' double envelopes
+          const DBox* p64 = F.tree[s.t].leaves64 + first;
+#pragma unroll
+          for (int c = 0; c < W; ++c)
+            if (((m >> c) & 1u) && !Ops::exact64(load_dbox(p64 + c), s.q)) m &= ~(1u << c);
+        } else if constexpr (Ops::kRefine) {
+#pragma unroll
+          for (int c = 0; c < W; ++c) {
+            const uint32_t idx = (static_cast<uint32_t>(c) + lane) & (W - 1);
+            if (((m >> idx) & 1u) && !Ops::exact(gl[idx], s.q)) m &= ~(1u << idx);
+          }
+        }
+        leafm = m;
+      } else {
+        s.ms.set(s.L, m);
+      }
+    }
+    if (MODE == kCollect) {
+      out.template add_resolved<W>(qu, leafm, S.sid[lane], s.qid + B.id_offset, s.rb);
+    } else {
+      cnt += __popc(leafm);
+    }
+    if (active) {
+      active = trav_advance<PRED, W>(F, s);
+      if (MODE == kCount && ROUTED && !active) {
+        count_routed(M, s.rb, cnt);
+        cnt = 0;
+      }
+    }
+    uint32_t idle = __ballot_sync(kFull, !active);
+    if (idle != 0 && next < cend) {
+      uint32_t slot = next + __popc(idle & lanemask_lt());
+      if (!active && slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
+      next = min(cend, next + __popc(idle));
+    }
+  }
+  if (MODE == kCollect) out.flush(qu);
+  if (MODE == kCount && !ROUTED) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
+  __syncwarp();
+  if (lane == 0) S.phase = phase;
+  __syncwarp();
+  return ok;
+}
+
+// ---------------------------------------------------------------------------
 // team scheme: W lanes per query, 32 / W queries in flight per warp (float
 // indexes only: double launches use the thread or packet scheme)
 // ---------------------------------------------------------------------------

@@ -58,3 +58,48 @@ def test_algorithmic_bytes_per_launch():
     assert bench.algorithmic_bytes(w, 5) == 16 * 10 + 16 * 3 + 8 * 5
     w["queries"], w["qwidth"] = np.zeros((3, 2), np.float32), 2
     assert bench.algorithmic_bytes(w, 0) == 16 * 10 + 8 * 3
+
+
+def _bench_layout(ora, kind, boxes, queries, sizes, rng):
+    """Per-batch results laid out as the bench's queues hold them: batch b's
+    pairs (query ids 0-based in the batch, in a shuffled order) at rows
+    [poffs[b], poffs[b] + count_b), one spare row for an empty batch."""
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    per = []
+    for b in range(len(sizes)):
+        _t, _c, p = ora.run(kind, boxes, queries[offs[b]:offs[b + 1]], grid=False)
+        per.append(p[rng.permutation(p.shape[0])])
+    counts = np.array([p.shape[0] for p in per], dtype=np.int64)
+    poffs = np.concatenate([[0], np.cumsum(np.maximum(counts, 1))])
+    pairs = np.full((int(poffs[-1]), 2), 0xDEADBEEF, dtype=np.uint32)
+    for b, p in enumerate(per):
+        pairs[poffs[b]:poffs[b] + p.shape[0]] = p
+    return pairs, counts, poffs
+
+
+def test_parity_check_accepts_the_oracles_pairs_and_catches_a_planted_mistake(oracle):
+    from rtspatial_b200 import workloads as wl
+    rng = np.random.default_rng(5)
+    boxes = wl.uniform_boxes(rng, 20_000, 3e-2)
+    queries = wl.uniform_boxes(rng, 900, 3e-2)
+    sizes = np.array([300, 0, 250, 350], dtype=np.int64)
+    for kind, name in ((1, "contains"), (2, "intersects")):
+        w = {"kind": name, "boxes": boxes, "queries": queries}
+        pairs, counts, poffs = _bench_layout(oracle, kind, boxes, queries, sizes, rng)
+        assert counts.sum() > 0
+        dig = bench.gpu_batch_digests(pairs, counts, poffs[:-1])
+        res = bench.oracle_batch_check(w, sizes, counts, dig)
+        assert res["equal"] and res["pairs"] == counts.sum(), res
+        # a missing pair (count and digest both change)
+        b = int(np.argmax(counts))
+        c2 = counts.copy()
+        c2[b] -= 1
+        dig2 = bench.gpu_batch_digests(pairs, c2, poffs[:-1])
+        res = bench.oracle_batch_check(w, sizes, c2, dig2)
+        assert not res["equal"] and res["mismatched_batches"] == [b]
+        # a wrong geom id at the right count (digest alone catches it)
+        p3 = pairs.copy()
+        p3[poffs[b], 0] ^= 1
+        dig3 = bench.gpu_batch_digests(p3, counts, poffs[:-1])
+        res = bench.oracle_batch_check(w, sizes, counts, dig3)
+        assert not res["equal"] and res["mismatched_batches"] == [b]
