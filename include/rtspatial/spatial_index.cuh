@@ -5,8 +5,14 @@
 // rtspatial::Exception on failure.  Link with -lrtspatial_b200.
 //
 // Handlers.  The reference picks its per-pair device handler when its shaders
-// are compiled (counting or collecting header).  Here Config::handler picks
-// one of the same two behaviours at run time; its default follows the macro
+// are compiled: RTSPATIAL_COMPILE_SHADERS force-includes a handler header and
+// Init loads the result from Config::ptx_root.  Here the same CMake function
+// (cmake/rtspatial_shaders.cmake) compiles a handler module with the header,
+// and Init loads <ptx_root>/rtspatial_handlers.cubin: queries then call the
+// header's rtspatial_handle_* functions once per pair (a module built from
+// the shipped counting or collecting header runs the library's own
+// warp-aggregated handler of that behaviour).  With ptx_root empty,
+// Config::handler picks a built-in behaviour; its default follows the macro
 // RTSPATIAL_COUNTING_HANDLERS (defined: counting, arg = unsigned long long*;
 // otherwise collecting, arg = dev::Queue<thrust::pair<uint32_t,uint32_t>>* in
 // device memory).
@@ -37,8 +43,11 @@
 
 namespace rtspatial {
 
+// File name of the handler module RTSPATIAL_COMPILE_SHADERS writes.
+constexpr const char* kHandlerModuleFile = "rtspatial_handlers.cubin";
+
 struct Config {
-  std::string ptx_root;  // no PTX modules to load; kept for source compatibility
+  std::string ptx_root;  // directory of the handler module (empty: built-in handler)
   size_t max_geometries = 1000 * 1000 * 10;
   size_t max_queries = 1000 * 1000;
   bool preallocate = false;
@@ -114,6 +123,11 @@ class SpatialIndex {
     if (h_) rts_destroy(h_);
     h_ = nullptr;
     RTS_CHECK(rts_create(&c, &h_));
+    if (!config.ptx_root.empty()) {
+      const std::string path = config.ptx_root + "/" + kHandlerModuleFile;
+      RTS_CHECK(rts_load_handler_module(h_, path.c_str()));
+      config_.handler = RTS_HANDLER_MODULE;
+    }
   }
 
   void Clear() { RTS_CHECK(rts_clear(handle(), nullptr)); }

@@ -48,7 +48,8 @@ extern "C" {
 /* ---- handlers ------------------------------------------------------------
  * The reference selects a device handler at shader compile time
  * (CMakeLists.txt:73-104 force-includes default_handlers/*.h).  Here the
- * handler is a run-time argument with the same two shipped behaviours:
+ * handler is a run-time argument: the same two shipped behaviours, built in,
+ * or the caller's own functions from a handler module (below):
  *  RTS_HANDLER_COUNT   arg = unsigned long long* in device memory; each pair
  *                      adds 1 (default_handlers/counting_handlers.h:7-25).
  *  RTS_HANDLER_COLLECT arg = rts_queue* in device memory; each pair is
@@ -59,6 +60,12 @@ extern "C" {
  *                      needed. */
 #define RTS_HANDLER_COUNT 0
 #define RTS_HANDLER_COLLECT 1
+/* RTS_HANDLER_MODULE  the caller's own rtspatial_handle_* device functions,
+ *                      called once per pair with `arg`, from the handler module
+ *                      loaded by rts_load_handler_module (the reference's
+ *                      compile-time handler header, CMakeLists.txt:73-104).
+ *                      Batches of one launch either all use it or none does. */
+#define RTS_HANDLER_MODULE 2
 
 /* thrust::pair<uint32_t, uint32_t> as the collecting handler writes it. */
 typedef struct rts_pair {
@@ -91,9 +98,10 @@ typedef struct rts_update_entry_f64 {
 
 /* ---- configuration ---------------------------------------------------------
  * First block: the fields of rtspatial::Config (spatial_index.cuh:22-37),
- * accepted for source compatibility.  ptx_root has no counterpart (there are
- * no PTX modules to load); the OptiX build flags and the intersects cost-model
- * fields do not change results and are ignored.
+ * accepted for source compatibility.  ptx_root is not a field here: the C++
+ * drop-in loads the handler module from it (rts_load_handler_module); the
+ * OptiX build flags and the intersects cost-model fields do not change results
+ * and are ignored.
  * Second block: this library's own structure and traversal knobs. */
 typedef struct rts_config {
   uint64_t max_geometries;      /* capacity reserved when preallocate != 0 */
@@ -354,6 +362,26 @@ int rts_server_reset_stats(rts_server* server);
 #define RTS_NOALLOC_MAX_BATCHES 1024
 int rts_query_batched_noalloc(rts_index* index, const rts_batch* batches, uint32_t n_batches,
                               void* stream);
+
+/* ---- handler modules ------------------------------------------------------
+ * Replaces the reference's shader build with the user's handler header
+ * (RTSPATIAL_COMPILE_SHADERS, CMakeLists.txt:73-104) and the PTX modules that
+ * SpatialIndex::Init loads from Config::ptx_root (spatial_index.cuh:83-87).
+ * The module is a cubin compiled from rtspatial_b200/shaders/
+ * rts_handler_module.cu with the handler header force-included
+ * (cmake/rtspatial_shaders.cmake, or python -m rtspatial_b200.handlers).  Loading
+ * it lets the index's queries take RTS_HANDLER_MODULE: the module's kernels
+ * walk the same tree and call rtspatial_handle_* once per pair.  A module built
+ * from the shipped counting or collecting header runs this library's own
+ * warp-aggregated handler of that behaviour instead (same results).  Loading
+ * another module replaces the previous one; the module stays loaded until the
+ * index is destroyed.  RTS_ERR_INVALID_ARGUMENT when the file is not a handler
+ * module of this library's version (its error names what was missing). */
+int rts_load_handler_module(rts_index* index, const char* cubin_path);
+/* The built-in handler a loaded module stands for (RTS_HANDLER_COUNT or
+ * RTS_HANDLER_COLLECT), or -1 when it calls the user's own functions or no
+ * module is loaded. */
+int rts_handler_module_builtin(const rts_index* index);
 
 /* ---- introspection ------------------------------------------------------ */
 uint64_t rts_size(const rts_index* index);       /* number of ids handed out */

@@ -25,6 +25,7 @@ RTS_PREDICATE_INTERSECTS = 0
 RTS_PREDICATE_CONTAINS = 1
 RTS_HANDLER_COUNT = 0
 RTS_HANDLER_COLLECT = 1
+RTS_HANDLER_MODULE = 2
 RTS_TRAVERSAL_AUTO = 0
 RTS_TRAVERSAL_THREAD = 1
 RTS_TRAVERSAL_TEAM = 2
@@ -139,6 +140,8 @@ SIGNATURES = {
     "rts_query_batched": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_query_batched_noalloc": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _P]),
     "rts_device_status": (_I, [_P, ctypes.POINTER(ctypes.c_uint32), _P]),
+    "rts_load_handler_module": (_I, [_P, ctypes.c_char_p]),
+    "rts_handler_module_builtin": (_I, [_P]),
     "rts_plan_create": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, ctypes.POINTER(_P)]),
     "rts_plan_launch": (_I, [_P, _P, _I]),
     "rts_plan_destroy": (_I, [_P]),

@@ -40,7 +40,15 @@ struct __align__(16) DBox {
 __device__ __forceinline__ DBox load_dbox(const DBox* p) {
   return DBox{__ldg(&p->lo), __ldg(&p->hi)};
 }
-enum HandlerKind : int { kCount = 0, kCollect = 1 };
+// kUser: the caller's own device handlers (rtspatial_handle_*), called once
+// per pair by the kernels of a handler module compiled with them.
+enum HandlerKind : int { kCount = 0, kCollect = 1, kUser = 2 };
+
+// Handler type of the kernels that do not call user handlers.
+struct NoUserHandler {
+  template <int PRED>
+  static __device__ __forceinline__ void call(uint32_t, uint32_t, void*) {}
+};
 
 // Two consecutive boxes with one 32-byte read-only load (sm_100 256-bit
 // vector load, four 64-bit lanes).  p must be 32-byte aligned: every W-group

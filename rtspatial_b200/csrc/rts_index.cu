@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "rts_handler_kernel.cuh"
 #include "rts_index_impl.h"
 
 namespace rts {
@@ -372,7 +373,7 @@ bool want_sort(const rts_index* ix, uint64_t total) {
 }
 
 bool merge_batches(const LaunchPlan& plan, const BatchDesc* descs, uint32_t nd) {
-  if (nd < 2 || plan.frontier || plan.team) return false;
+  if (nd < 2 || plan.frontier || plan.team || plan.user_kernel) return false;
   for (uint32_t i = 1; i < nd; ++i)
     if (descs[i].pred != descs[0].pred || descs[i].mode != descs[0].mode) return false;
   // Measured on B200: routing pays for counting and for the packet scheme
@@ -444,8 +445,9 @@ int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
 int batch_desc(const rts_index* ix, const rts_batch& b, const LaunchPlan& plan, uint64_t& chunks,
                uint64_t& qsum, BatchDesc& d, bool* keep) {
   *keep = false;
-  int rc;
+  int rc, mode;
   if ((rc = check_handler(b.handler, b.arg))) return rc;
+  if ((rc = resolve_handler(ix, b.handler, &mode))) return rc;
   int pred;
   const bool f64 = b.query_kind == RTS_QUERY_POINTS_F64 || b.query_kind == RTS_QUERY_ENVELOPES_F64;
   if (b.query_kind == RTS_QUERY_POINTS || b.query_kind == RTS_QUERY_POINTS_F64) {
@@ -470,7 +472,7 @@ int batch_desc(const rts_index* ix, const rts_batch& b, const LaunchPlan& plan, 
   d.arg = b.arg;
   d.n = static_cast<uint32_t>(b.n);
   d.pred = pred;
-  d.mode = b.handler;
+  d.mode = mode;
   d.chunk_begin = static_cast<uint32_t>(chunks);
   d.order = nullptr;
   d.qbase = static_cast<uint32_t>(qsum);
@@ -581,9 +583,39 @@ uint64_t sum_queries(const rts_batch* batches, uint32_t n) {
 }
 
 int check_handler(int handler, void* arg) {
-  if (handler != RTS_HANDLER_COUNT && handler != RTS_HANDLER_COLLECT)
+  if (handler != RTS_HANDLER_COUNT && handler != RTS_HANDLER_COLLECT &&
+      handler != RTS_HANDLER_MODULE)
     return fail(RTS_ERR_INVALID_ARGUMENT, "unknown handler");
   if (!arg) return fail(RTS_ERR_INVALID_ARGUMENT, "handler argument is null");
+  return RTS_OK;
+}
+
+// The kernel-side handler of a public handler kind: a loaded module built
+// from a shipped handler header stands for the built-in handler of the same
+// behaviour; any other module is called per pair (kUser).
+int resolve_handler(const rts_index* ix, int handler, int* mode) {
+  if (handler != RTS_HANDLER_MODULE) {
+    *mode = handler;
+    return RTS_OK;
+  }
+  if (!ix->hmod)
+    return fail(RTS_ERR_INVALID_ARGUMENT,
+                "RTS_HANDLER_MODULE without a loaded handler module (rts_load_handler_module)");
+  *mode = ix->hmod_builtin >= 0 ? ix->hmod_builtin : kUser;
+  return RTS_OK;
+}
+
+int handler_plan(const rts_index* ix, const BatchDesc* descs, uint32_t nd, LaunchPlan& plan) {
+  uint32_t user = 0;
+  for (uint32_t i = 0; i < nd; ++i) user += descs[i].mode == kUser;
+  if (user == 0) return RTS_OK;
+  if (user != nd)
+    return fail(RTS_ERR_INVALID_ARGUMENT,
+                "batches with the handler module and with built-in handlers in one launch");
+  const int slot = ix->W == 4 ? 0 : ix->W == 8 ? 1 : ix->W == 16 ? 2 : 3;
+  plan.user_kernel = reinterpret_cast<const void*>(ix->hkern[slot]);
+  plan.team = plan.packet = plan.frontier = plan.staged = false;
+  plan.merged = false;
   return RTS_OK;
 }
 
@@ -591,6 +623,8 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
               cudaStream_t s) {
   int rc = check_handler(handler, arg);
   if (rc) return rc;
+  int mode;
+  if ((rc = resolve_handler(ix, handler, &mode))) return rc;
   if (n == 0 || ix->n_ids == 0) return RTS_OK;  // spatial_index.cuh:354-356
   if (!q) return fail(RTS_ERR_INVALID_ARGUMENT, "queries is null");
   if (n > 0xffffffffull) return fail(RTS_ERR_CAPACITY, "more than 2^32-1 queries in one call");
@@ -601,11 +635,12 @@ int query_one(rts_index* ix, int pred, const float* q, uint64_t n, int handler, 
   b.arg = arg;
   b.n = static_cast<uint32_t>(n);
   b.pred = pred;
-  b.mode = handler;
+  b.mode = mode;
   b.chunk_begin = 0;
   b.order = nullptr;
   b.qbase = 0;
   LaunchPlan plan = plan_for(ix, pred, n);
+  if ((rc = handler_plan(ix, &b, 1, plan))) return rc;
   if (want_sort(ix, n)) {
     const uint64_t chunks = (n + plan.chunk - 1) / plan.chunk;
     if ((rc = plan_order(ix->qs, plan, &b, 1, n, chunks, s))) return rc;
@@ -700,6 +735,10 @@ int rts_destroy(rts_index* ix) {
   }
   if (ix->ev_rebuild0) cudaEventDestroy(ix->ev_rebuild0);
   if (ix->ev_rebuild1) cudaEventDestroy(ix->ev_rebuild1);
+  if (ix->hmod) {
+    cudaDeviceSynchronize();  // no launch of its kernels may still run
+    cudaLibraryUnload(ix->hmod);
+  }
   touched |= ix->qs.work.ptr != nullptr;
   ix->qs.release(s);
   ix->staging.release();
@@ -924,6 +963,7 @@ int rts_query_batched(rts_index* ix, const rts_batch* batches, uint32_t n_batche
   uint64_t chunks = 0;
   int rc = make_descs(ix, batches, n_batches, plan, descs, chunks);
   if (rc) return rc;
+  if ((rc = handler_plan(ix, descs.data(), static_cast<uint32_t>(descs.size()), plan))) return rc;
   if (descs.empty() || ix->n_ids == 0) return RTS_OK;
   if ((rc = refresh_forest(ix))) return rc;
   if ((rc = buf_reserve(ix->qs.work, sizeof(uint32_t), s, false, 0))) return rc;
@@ -977,6 +1017,55 @@ int rts_report_query_time(rts_index* ix, double query_ms, float* rebuild_update_
   }
   if (rebuild_update_fraction) *rebuild_update_fraction = ix->cfg.rebuild_update_fraction;
   return RTS_OK;
+}
+
+int rts_load_handler_module(rts_index* ix, const char* path) {
+  if (!ix || !path) return fail(RTS_ERR_INVALID_ARGUMENT, "index or path is null");
+  cudaLibrary_t lib = nullptr;
+  cudaError_t e = cudaLibraryLoadFromFile(&lib, path, nullptr, nullptr, 0, nullptr, nullptr, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RTS_ERR_INVALID_ARGUMENT,
+                std::string("cannot load handler module ") + path + ": " + cudaGetErrorString(e));
+  }
+  auto reject = [&](const std::string& why) {
+    cudaLibraryUnload(lib);
+    cudaGetLastError();
+    return fail(RTS_ERR_INVALID_ARGUMENT, std::string("handler module ") + path + ": " + why);
+  };
+  int vals[2] = {0, 0};
+  const char* globals[2] = {"rts_module_abi_version", "rts_module_builtin_handler"};
+  for (int i = 0; i < 2; ++i) {
+    void* d = nullptr;
+    size_t bytes = 0;
+    if (cudaLibraryGetGlobal(&d, &bytes, lib, globals[i]) != cudaSuccess || bytes != sizeof(int))
+      return reject(std::string("no ") + globals[i]);
+    if (cudaMemcpy(&vals[i], d, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return reject(std::string("cannot read ") + globals[i]);
+  }
+  if (vals[0] != kHandlerModuleAbi)
+    return reject("built for module version " + std::to_string(vals[0]) + ", the library reads " +
+                  std::to_string(kHandlerModuleAbi));
+  cudaKernel_t k[4] = {};
+  const int widths[4] = {4, 8, 16, 32};
+  for (int i = 0; i < 4; ++i) {
+    const std::string name = "rts_handler_query_v" + std::to_string(kHandlerModuleAbi) + "_w" +
+                             std::to_string(widths[i]);
+    if (cudaLibraryGetKernel(&k[i], lib, name.c_str()) != cudaSuccess)
+      return reject("no kernel " + name);
+  }
+  if (ix->hmod) {
+    cudaDeviceSynchronize();
+    cudaLibraryUnload(ix->hmod);
+  }
+  ix->hmod = lib;
+  for (int i = 0; i < 4; ++i) ix->hkern[i] = k[i];
+  ix->hmod_builtin = (vals[1] == RTS_HANDLER_COUNT || vals[1] == RTS_HANDLER_COLLECT) ? vals[1] : -1;
+  return RTS_OK;
+}
+
+int rts_handler_module_builtin(const rts_index* ix) {
+  return (ix && ix->hmod) ? ix->hmod_builtin : -1;
 }
 
 int rts_device_status(rts_index* ix, uint32_t* status, void* stream) {
@@ -1086,6 +1175,7 @@ extern "C" int rts_query_batched_noalloc(rts_index* ix, const rts_batch* batches
                                         " non-empty batches per call");
     descs[nd++] = d;
   }
+  if ((rc = handler_plan(ix, descs, nd, plan))) return rc;
   if (nd == 0 || ix->n_ids == 0) return RTS_OK;
   void* scratch = nullptr;
   if ((rc = noalloc_scratch(&scratch))) return rc;

@@ -92,6 +92,11 @@ struct rts_index {
   uint64_t version = 0;         // bumped when buffers or sub-trees change
   rts::DevBuf leaves, leaf_ids, pos;
   rts::DevBuf status;           // device status word: kErr* bits set by query kernels
+  // handler module (rts_load_handler_module): its kernels per node width 4, 8,
+  // 16, 32, and the built-in handler it stands for (-1: the user's functions)
+  cudaLibrary_t hmod = nullptr;
+  cudaKernel_t hkern[4] = {};
+  int hmod_builtin = -1;
   rts::DevBuf leaves64;         // double index: the double envelopes, slot by slot
   rts::DevBuf rounded;          // double index: scratch of an insert's float rounding
   // scratch of the update split: slot bitmaps, moved ids / envelopes, count
@@ -134,6 +139,8 @@ int launch_pred(const rts_batch* batches, uint32_t n);
 void keep_pool_memory();
 bool want_sort(const rts_index* ix, uint64_t total);
 int check_handler(int handler, void* arg);
+// The kernel-side handler (kCount, kCollect or kUser) of a public handler kind.
+int resolve_handler(const rts_index* ix, int handler, int* mode);
 // Whether a sorted launch of these batches runs merged: more than one batch,
 // all of one predicate and handler, the thread or packet scheme, and either
 // the counting handler or the packet scheme.
@@ -147,6 +154,10 @@ int fill_order(rts_index* ix, QueryScratch& qs, const LaunchPlan& plan, const Ba
                const BatchDesc* dev, uint32_t nd, uint64_t total, uint64_t chunks, cudaStream_t s);
 int make_descs(const rts_index* ix, const rts_batch* batches, uint32_t n_batches,
                const LaunchPlan& plan, std::vector<BatchDesc>& out, uint64_t& chunks);
+// The launch of batches with the caller's handler module (mode kUser): every
+// batch must use it; the plan then runs the module's thread-scheme kernel at
+// the index's node width, batch by batch.  No-op for built-in handlers.
+int handler_plan(const rts_index* ix, const BatchDesc* descs, uint32_t nd, LaunchPlan& plan);
 // Sizes the frontier buffers of `qs` for `total` queries (no-op when large
 // enough); fills qs.fb.
 int reserve_frontier(rts_index* ix, QueryScratch& qs, uint64_t total, cudaStream_t s);

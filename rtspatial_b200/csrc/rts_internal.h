@@ -154,6 +154,7 @@ struct LaunchPlan {
   bool frontier = false;      // breadth-first pass (plus depth-first fallback)
   bool packet = false;        // warp-per-packet depth-first scheme
   bool staged = false;        // thread scheme with groups bulk-copied into shared memory
+  const void* user_kernel = nullptr;  // handler module's kernel (cudaKernel_t) for kUser batches
   uint32_t chunk = 32;  // queries per work item
   int min_blocks = 1;         // CTAs of 256 threads per SM the registers are capped for (1-4)
   bool merged = false;        // sort the queries of all batches together (MergedOrder)

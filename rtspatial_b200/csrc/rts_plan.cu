@@ -66,6 +66,8 @@ int rts_plan_create(rts_index* ix, const rts_batch* batches, uint32_t n_batches,
   p->plan = plan_for(ix, launch_pred(batches, n_batches),
                      n_batches ? sum_queries(batches, n_batches) : 0);
   int rc = make_descs(ix, batches, n_batches, p->plan, p->descs, p->chunks);
+  if (!rc)
+    rc = handler_plan(ix, p->descs.data(), static_cast<uint32_t>(p->descs.size()), p->plan);
   cudaStream_t s = 0;
   for (const auto& d : p->descs) p->total += d.n;
   if (!rc) rc = buf_reserve(p->qs.work, sizeof(uint32_t), s, false, 0);

@@ -79,6 +79,7 @@ static int prepare_kernel(QueryKernel k, size_t dyn) {
 }
 
 int prepare_query_kernel(const LaunchPlan& plan) {
+  if (plan.user_kernel) return RTS_OK;
   QueryKernel k = pick_kernel(plan, plan.merged);
   return k ? prepare_kernel(k, dyn_smem_bytes(plan, plan.merged)) : RTS_OK;
 }
@@ -103,6 +104,33 @@ int launch_queries(const Forest& F, const LaunchPlan& plan, const BatchDesc* hb,
                    const uint32_t* only_any, const MergedOrder* merged,
                    const uint32_t* chunk_order) {
   if (total_chunks == 0) return RTS_OK;
+  if (plan.user_kernel) {  // the caller's handler module: its kernel, same arguments
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan.user_kernel, kQueryThreads,
+                                                      0) != cudaSuccess ||
+        per_sm <= 0) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    const uint64_t want = (static_cast<uint64_t>(total_chunks) + kQueryThreads / 32 - 1) /
+                          (kQueryThreads / 32);
+    const uint64_t cap = static_cast<uint64_t>(device_sm_count()) * per_sm;
+    const unsigned grid = static_cast<unsigned>(want < cap ? want : cap);
+    RTS_CUDA_TRY(cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), s));
+    Forest F_arg = F;
+    BatchDesc b0 = hb[0];
+    const BatchDesc* d_arg = db;
+    uint32_t nb_arg = nb, tc_arg = total_chunks, chunk_arg = plan.chunk;
+    uint32_t* work_arg = work_counter;
+    const uint32_t* only_arg = only;
+    const uint32_t* only_any_arg = only_any;
+    MergedOrder M{nullptr, nullptr, nullptr, nullptr};
+    const uint32_t* order_arg = chunk_order;
+    void* args[] = {&F_arg, &b0, &d_arg, &nb_arg, &tc_arg, &chunk_arg, &work_arg,
+                    &only_arg, &only_any_arg, &M, &order_arg};
+    RTS_CUDA_TRY(cudaLaunchKernel(plan.user_kernel, dim3(grid), dim3(kQueryThreads), args, 0, s));
+    return RTS_OK;
+  }
   LaunchPlan use = plan;
   if (only) use.packet = false;  // the packet scheme takes no query filter
   if (use.staged && use.width > 16) use.staged = false;  // slots hold at most 16 boxes

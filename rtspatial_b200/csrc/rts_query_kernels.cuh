@@ -27,14 +27,23 @@ __device__ __forceinline__ void run_chunk(const Forest& F, const BatchDesc& B, u
   }
 }
 
-// Not inlined (twelve predicate / handler bodies per kernel), so instantiated
-// per MINB: a called function is register-allocated once, for the tightest
-// budget among the kernels that call it.
+// Every predicate / handler body is its own function, not inlined: a
+// function is register-allocated once, for its own needs (twelve bodies in one
+// function were allocated for their union and spilled), and for the tightest
+// budget among the kernels that call it, so the bodies are instantiated per
+// MINB.  A body is called once per chunk of queries.
+template <int W, bool TEAM, bool ROUTED, int MINB, int PRED, int MODE>
+__device__ __noinline__ void chunk_body(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                        uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                        const uint32_t* only, const MergedOrder& M) {
+  run_chunk<W, TEAM, ROUTED, PRED, MODE>(F, B, cb, ce, wbuf, wbat, only, M);
+}
+
 template <int W, bool TEAM, bool ROUTED, int MINB>
-__device__ __noinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                            uint32_t ce, DevPair* wbuf, uint32_t* wbat,
-                                            const uint32_t* only, const MergedOrder& M) {
-#define RTS_RUN(P, H) run_chunk<W, TEAM, ROUTED, P, H>(F, B, cb, ce, wbuf, wbat, only, M)
+__device__ __forceinline__ void dispatch_chunk(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                               uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                               const uint32_t* only, const MergedOrder& M) {
+#define RTS_RUN(P, H) chunk_body<W, TEAM, ROUTED, MINB, P, H>(F, B, cb, ce, wbuf, wbat, only, M)
   switch (B.pred * 2 + B.mode) {
     case kPoint * 2 + kCount: RTS_RUN(kPoint, kCount); break;
     case kPoint * 2 + kCollect: RTS_RUN(kPoint, kCollect); break;
@@ -105,11 +114,18 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
   }
 }
 
-template <int W, bool ROUTED, int MINB>  // per MINB, as dispatch_chunk
-__device__ __noinline__ void dispatch_packet(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                             uint32_t ce, DevPair* wbuf, uint32_t* wbat,
-                                             void* praw, const MergedOrder& M) {
-#define RTS_RUN(P, H) run_chunk_packet<P, H, W, ROUTED>(F, B, cb, ce, wbuf, wbat, praw, M)
+template <int W, bool ROUTED, int MINB, int PRED, int MODE>  // per body, as chunk_body
+__device__ __noinline__ void packet_body(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                         uint32_t ce, DevPair* wbuf, uint32_t* wbat, void* praw,
+                                         const MergedOrder& M) {
+  run_chunk_packet<PRED, MODE, W, ROUTED>(F, B, cb, ce, wbuf, wbat, praw, M);
+}
+
+template <int W, bool ROUTED, int MINB>
+__device__ __forceinline__ void dispatch_packet(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                                uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                                void* praw, const MergedOrder& M) {
+#define RTS_RUN(P, H) packet_body<W, ROUTED, MINB, P, H>(F, B, cb, ce, wbuf, wbat, praw, M)
   switch (B.pred * 2 + B.mode) {
     case kPoint * 2 + kCount: RTS_RUN(kPoint, kCount); break;
     case kPoint * 2 + kCollect: RTS_RUN(kPoint, kCollect); break;
@@ -186,12 +202,20 @@ __global__ void __launch_bounds__(kQueryThreads, MINB)
 // Staged scheme (run_chunk_staged): per warp, one StageWarp<W> area at the
 // start of the dynamic shared memory, then (merged launch) the warps' batch
 // tables.  Returns false when a copy wait gave up (the kernel then stops).
+template <int W, bool ROUTED, int PRED, int MODE>  // per body, as chunk_body
+__device__ __noinline__ bool staged_body(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                         uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                         const uint32_t* only, const MergedOrder& M,
+                                         StageWarp<W>& S) {
+  return run_chunk_staged<PRED, MODE, W, ROUTED>(F, B, cb, ce, wbuf, wbat, only, M, S);
+}
+
 template <int W, bool ROUTED>
-__device__ __noinline__ bool dispatch_staged(const Forest& F, const BatchDesc& B, uint32_t cb,
-                                             uint32_t ce, DevPair* wbuf, uint32_t* wbat,
-                                             const uint32_t* only, const MergedOrder& M,
-                                             StageWarp<W>& S) {
-#define RTS_RUN(P, H) return run_chunk_staged<P, H, W, ROUTED>(F, B, cb, ce, wbuf, wbat, only, M, S)
+__device__ __forceinline__ bool dispatch_staged(const Forest& F, const BatchDesc& B, uint32_t cb,
+                                                uint32_t ce, DevPair* wbuf, uint32_t* wbat,
+                                                const uint32_t* only, const MergedOrder& M,
+                                                StageWarp<W>& S) {
+#define RTS_RUN(P, H) return staged_body<W, ROUTED, P, H>(F, B, cb, ce, wbuf, wbat, only, M, S)
   switch (B.pred * 2 + B.mode) {
     case kPoint * 2 + kCount: RTS_RUN(kPoint, kCount);
     case kPoint * 2 + kCollect: RTS_RUN(kPoint, kCollect);

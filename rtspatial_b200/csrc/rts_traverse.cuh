@@ -1,13 +1,15 @@
 // Traversal of the implicit W-wide forest, one warp at a time.
 //
-// Two warp-level schemes over the same layout:
+// Warp-level schemes over the same layout:
 //  - thread: each lane owns one query and tests a whole group of W children
 //    per step (W float4 loads, W predicate evaluations);
+//  - staged: the thread scheme with each group bulk-copied into shared memory;
 //  - team:   W lanes own one query and each tests one child per step (one
-//    coalesced 16*W-byte load per team, a ballot builds the child mask).
-// Both keep, per query, the child masks of every level on the way down
-// (MaskStack) instead of a pointer stack: descending takes the lowest set bit
-// of the current level's mask; ascending divides the group index by W.
+//    coalesced 16*W-byte load per team, a ballot builds the child mask);
+//  - packet: one warp walks up to 32 queries together, one entry per lane.
+// All keep, per query (or packet), the child masks of every level on the way
+// down (MaskStack) instead of a pointer stack: descending takes the lowest set
+// bit of the current level's mask; ascending divides the group index by W.
 //
 // A warp works through a chunk [cbeg, cend) of one batch's queries.  Lanes
 // (or teams) whose query is finished take the next unstarted query of the
@@ -89,7 +91,9 @@ __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>
 // ---------------------------------------------------------------------------
 // thread scheme
 // ---------------------------------------------------------------------------
-template <int PRED, int MODE, int W, bool ROUTED>
+// MODE kUser: H::call<PRED>(geom_id, query_id, arg) once per pair, the
+// reference's per-hit handler contract (ROUTED false).
+template <int PRED, int MODE, int W, bool ROUTED, class H = NoUserHandler>
 __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDesc& B,
                                                  uint32_t cbeg, uint32_t cend, DevPair* wbuf, uint32_t* wbat,
                                                  const uint32_t* only,
@@ -152,8 +156,13 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
         s.ms.set(s.L, m);
       }
     }
-    if (MODE == kCollect) {
+    if constexpr (MODE == kCollect) {
       out.template add<W>(qu, leafm, leafslot, s.qid + B.id_offset, s.rb);
+    } else if constexpr (MODE == kUser) {
+      for (uint32_t m = leafm; m; m &= m - 1) {
+        const uint32_t c = __ffs(m) - 1;
+        H::template call<PRED>(__ldg(F.ids_base + leafslot + c), s.qid + B.id_offset, B.arg);
+      }
     } else {
       cnt += __popc(leafm);
     }
@@ -172,8 +181,9 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       next = min(cend, next + __popc(idle));
     }
   }
-  if (MODE == kCollect) out.flush(qu);
-  if (MODE == kCount && !ROUTED) count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
+  if constexpr (MODE == kCollect) out.flush(qu);
+  if constexpr (MODE == kCount && !ROUTED)
+    count_flush_warp(static_cast<unsigned long long*>(B.arg), cnt);
 }
 
 // ---------------------------------------------------------------------------

@@ -143,6 +143,9 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
       {RTS_TRAVERSAL_PACKET, 1, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 64},
       {RTS_TRAVERSAL_PACKET, 2, 1, 64},   {RTS_TRAVERSAL_PACKET, 4, 1, 256},
       {RTS_TRAVERSAL_PACKET, 3, 1, 64},
+      // staged: the occupancy field does not apply (shared memory sets it)
+      {RTS_TRAVERSAL_STAGED, 1, 1, 64},   {RTS_TRAVERSAL_STAGED, 1, 1, 128},
+      {RTS_TRAVERSAL_STAGED, 1, 0, 128},  {RTS_TRAVERSAL_STAGED, 1, 1, 256},
   };
   double best = 1e300, first = -1;
   int best_w = ix->W;
@@ -151,7 +154,8 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
   for (int W : widths) {
     if ((rc = rebuild_at_width(ix, W, s))) break;
     for (const Candidate& c : cands) {
-      if (c.traversal == RTS_TRAVERSAL_THREAD && W > 16) continue;  // W float4 per lane
+      if ((c.traversal == RTS_TRAVERSAL_THREAD || c.traversal == RTS_TRAVERSAL_STAGED) && W > 16)
+        continue;  // W float4 per lane
       ix->cfg.traversal = c.traversal;
       ix->cfg.query_occupancy = c.occupancy;
       ix->cfg.sort_queries = c.sort;

@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import ctypes
 import enum
+import os
 from dataclasses import dataclass, fields
 from typing import Iterable, Sequence
 
@@ -47,10 +48,12 @@ class Predicate(enum.IntEnum):
 
 
 class Handler(enum.IntEnum):
-    """The two shipped handler headers (default_handlers/*.h)."""
+    """The two shipped handler headers (default_handlers/*.h), and the
+    caller's own rtspatial_handle_* functions from a loaded handler module."""
 
     COUNT = L.RTS_HANDLER_COUNT
     COLLECT = L.RTS_HANDLER_COLLECT
+    MODULE = L.RTS_HANDLER_MODULE
 
 
 @dataclass
@@ -310,6 +313,24 @@ class SpatialIndex:
         """A prepared launch of fixed batches, replayable through a CUDA graph
         (``rts_plan_*``).  Query tensors and outputs must stay allocated."""
         return Plan(self, batches)
+
+    def load_handler_module(self, path: str) -> None:
+        """Loads a handler module (``rtspatial_b200.handlers.compile_module``):
+        queries with ``Handler.MODULE`` then call its rtspatial_handle_*
+        functions once per pair."""
+        check(lib().rts_load_handler_module(self._handle(), os.fsencode(path)))
+
+    def handler_module_builtin(self) -> int:
+        """RTS_HANDLER_COUNT / RTS_HANDLER_COLLECT when the loaded module was
+        built from a shipped handler header, else -1."""
+        return int(lib().rts_handler_module_builtin(self._handle()))
+
+    def device_status(self, stream=None) -> int:
+        """The index's device status bits (RTS_STATUS_*); 0 when every launch
+        completed normally."""
+        st = ctypes.c_uint32()
+        check(lib().rts_device_status(self._handle(), ctypes.byref(st), _stream_handle(stream)))
+        return int(st.value)
 
     def report_query_time(self, ms: float) -> float:
         """Feeds the refit-vs-rebuild tuner; returns the new re-sort threshold."""

@@ -12,7 +12,7 @@ from rtspatial_b200 import _lib as L
 
 WIDTHS = (4, 8, 16, 32)
 TRAVERSALS = (L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_TEAM, L.RTS_TRAVERSAL_FRONTIER,
-              L.RTS_TRAVERSAL_PACKET)
+              L.RTS_TRAVERSAL_PACKET, L.RTS_TRAVERSAL_STAGED)
 CURVES = (L.RTS_CURVE_MORTON, L.RTS_CURVE_HILBERT)
 
 # every (width, traversal, curve) combination
@@ -25,7 +25,8 @@ SOME_COMBOS = [(w, t, CURVES[i % 2]) for i, (w, t) in
 def combo_id(c):
     w, t, cu = c
     tn = {L.RTS_TRAVERSAL_THREAD: "thread", L.RTS_TRAVERSAL_TEAM: "team",
-          L.RTS_TRAVERSAL_FRONTIER: "frontier", L.RTS_TRAVERSAL_PACKET: "packet"}[t]
+          L.RTS_TRAVERSAL_FRONTIER: "frontier", L.RTS_TRAVERSAL_PACKET: "packet",
+          L.RTS_TRAVERSAL_STAGED: "staged"}[t]
     return f"w{w}-{tn}-" \
            f"{'morton' if cu == L.RTS_CURVE_MORTON else 'hilbert'}"
 

@@ -90,7 +90,7 @@ def test_argument_validation_without_gpu():
     c.max_trees = 8
     # every traversal scheme the header defines is accepted at creation
     for t in (L.RTS_TRAVERSAL_AUTO, L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_TEAM,
-              L.RTS_TRAVERSAL_FRONTIER, L.RTS_TRAVERSAL_PACKET):
+              L.RTS_TRAVERSAL_FRONTIER, L.RTS_TRAVERSAL_PACKET, L.RTS_TRAVERSAL_STAGED):
         c.traversal = t
         h2 = ctypes.c_void_p()
         assert lib.rts_create(ctypes.byref(c), ctypes.byref(h2)) == L.RTS_OK, t

@@ -58,7 +58,7 @@ def scene():
 
 SCHEMES = [(16, L.RTS_TRAVERSAL_THREAD), (8, L.RTS_TRAVERSAL_THREAD), (32, L.RTS_TRAVERSAL_PACKET),
            (16, L.RTS_TRAVERSAL_PACKET), (4, L.RTS_TRAVERSAL_AUTO), (16, L.RTS_TRAVERSAL_TEAM),
-           (8, L.RTS_TRAVERSAL_FRONTIER)]
+           (8, L.RTS_TRAVERSAL_FRONTIER), (16, L.RTS_TRAVERSAL_STAGED), (4, L.RTS_TRAVERSAL_STAGED)]
 
 
 def make(w, t, **kw):
@@ -79,7 +79,8 @@ def test_double_queries_match_oracle(cuda, oracle, scene, w, t):
         assert ix.query_count(KINDS[kind][1], ddev(src)) == want.shape[0]
 
 
-@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET])
+@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET,
+                               L.RTS_TRAVERSAL_STAGED])
 def test_double_delete_and_update(cuda, oracle, scene, t):
     boxes, pts, qs = scene
     rng = np.random.default_rng(65)
@@ -108,7 +109,8 @@ def test_double_delete_and_update(cuda, oracle, scene, t):
                           oracle.run64(KINDS[kind][0], cur, src)[2], f"after re-sort {kind}")
 
 
-@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET])
+@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET,
+                               L.RTS_TRAVERSAL_STAGED])
 def test_double_batched_merged_and_planned(cuda, oracle, scene, t):
     boxes, pts, qs = scene
     ix = make(16, t, sort_queries=1)
@@ -162,7 +164,8 @@ def test_double_server(cuda, oracle, scene):
     sv.close()
 
 
-@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET])
+@pytest.mark.parametrize("t", [L.RTS_TRAVERSAL_THREAD, L.RTS_TRAVERSAL_PACKET,
+                               L.RTS_TRAVERSAL_STAGED])
 def test_double_emptied_slots_match_no_query(cuda, oracle, scene, t):
     # Slots emptied by updates that move envelopes to a new sub-tree answer
     # nothing, including queries with infinite coordinates.

@@ -90,8 +90,8 @@ def test_merged_overflow_is_per_batch(cuda, oracle, scene):
 
 @pytest.mark.parametrize("w", [4, 8, 16, 32])
 @pytest.mark.parametrize("traversal", [rb._lib.RTS_TRAVERSAL_THREAD, rb._lib.RTS_TRAVERSAL_TEAM,
-                                       rb._lib.RTS_TRAVERSAL_PACKET],
-                         ids=["thread", "team", "packet"])
+                                       rb._lib.RTS_TRAVERSAL_PACKET, rb._lib.RTS_TRAVERSAL_STAGED],
+                         ids=["thread", "team", "packet", "staged"])
 def test_dense_hits_bypass_the_warp_buffer(cuda, oracle, w, traversal):
     # Every query lies in every box: a warp step finds more pairs than its
     # staging buffer holds and writes them straight to each batch's queue;
@@ -147,8 +147,9 @@ def test_merged_plan_graph_replay(cuda, oracle, scene):
     plan.close()
 
 
-@pytest.mark.parametrize("traversal", [rb._lib.RTS_TRAVERSAL_THREAD, rb._lib.RTS_TRAVERSAL_PACKET],
-                         ids=["thread", "packet"])
+@pytest.mark.parametrize("traversal", [rb._lib.RTS_TRAVERSAL_THREAD, rb._lib.RTS_TRAVERSAL_PACKET,
+                                       rb._lib.RTS_TRAVERSAL_STAGED],
+                         ids=["thread", "packet", "staged"])
 def test_merged_many_batches_fill_the_route_table(cuda, oracle, scene, traversal):
     # 300 batches of 20 queries, interleaved by the launch-wide sort: a flush
     # holds pairs of more batches than its table has slots.

@@ -90,8 +90,8 @@ def test_deleted_box_semantics(cuda, oracle):
 
 
 @pytest.mark.parametrize("w,t", [(16, rb._lib.RTS_TRAVERSAL_THREAD), (32, rb._lib.RTS_TRAVERSAL_PACKET),
-                                 (8, rb._lib.RTS_TRAVERSAL_TEAM)], ids=["w16-thread", "w32-packet",
-                                                                        "w8-team"])
+                                 (8, rb._lib.RTS_TRAVERSAL_TEAM), (16, rb._lib.RTS_TRAVERSAL_STAGED)],
+                         ids=["w16-thread", "w32-packet", "w8-team", "w16-staged"])
 def test_update_moves_far_envelopes_to_a_new_subtree(cuda, oracle, w, t):
     # Updates to random far positions leave their leaf group: their slots are
     # emptied and they move (same ids) into a new sub-tree; small moves stay.
@@ -129,8 +129,8 @@ def test_update_moves_far_envelopes_to_a_new_subtree(cuda, oracle, w, t):
 
 @pytest.mark.parametrize("w,t", [(16, rb._lib.RTS_TRAVERSAL_THREAD), (32, rb._lib.RTS_TRAVERSAL_PACKET),
                                  (8, rb._lib.RTS_TRAVERSAL_TEAM),
-                                 (8, rb._lib.RTS_TRAVERSAL_FRONTIER)],
-                         ids=["w16-thread", "w32-packet", "w8-team", "w8-frontier"])
+                                 (8, rb._lib.RTS_TRAVERSAL_FRONTIER), (8, rb._lib.RTS_TRAVERSAL_STAGED)],
+                         ids=["w16-thread", "w32-packet", "w8-team", "w8-frontier", "w8-staged"])
 def test_emptied_slots_match_no_query(cuda, oracle, w, t):
     # A slot emptied by a move keeps its id; it must not answer any query, not
     # even the inverted infinite envelope that every stored box contains
