@@ -518,7 +518,44 @@ struct MaskStack {
     for (int i = 0; i < kWords; ++i)
       if (i == wi) w[i] = (w[i] & ~(kMask << sh)) | (static_cast<uint64_t>(m) << sh);
   }
+  __device__ __forceinline__ bool any() const {
+    uint64_t v = 0;
+#pragma unroll
+    for (int i = 0; i < kWords; ++i) v |= w[i];
+    return v != 0;
+  }
+  // Clears the highest set bit and returns its index p (level p / W + 1, entry
+  // p % W of its group): a pending entry of the shallowest pending level, the
+  // largest sub-tree still to walk.  -1 when empty.
+  __device__ __forceinline__ int pop_highest() {
+#pragma unroll
+    for (int i = kWords - 1; i >= 0; --i) {
+      if (w[i] != 0) {
+        const int b = 63 - __clzll(static_cast<long long>(w[i]));
+        w[i] &= ~(1ull << b);
+        return b + 64 * i;
+      }
+    }
+    return -1;
+  }
 };
+
+template <int W>
+constexpr uint32_t log2_width() {
+  return W == 4 ? 2u : W == 8 ? 3u : W == 16 ? 4u : 5u;
+}
+
+// v as lane `src` holds it, for any struct of 32-bit words.
+template <class T>
+__device__ __forceinline__ T shfl_words(const T& v, int src) {
+  static_assert(sizeof(T) % 4 == 0, "whole 32-bit words");
+  T out;
+  const uint32_t* a = reinterpret_cast<const uint32_t*>(&v);
+  uint32_t* b = reinterpret_cast<uint32_t*>(&out);
+#pragma unroll
+  for (int i = 0; i < static_cast<int>(sizeof(T) / 4); ++i) b[i] = __shfl_sync(kFull, a[i], src);
+  return out;
+}
 
 // ---------------------------------------------------------------------------
 // Output: the two handler behaviours, warp-aggregated.

@@ -23,6 +23,9 @@
 
 namespace rts {
 
+// ceil of a lane that walks a whole query (every sub-tree of the forest).
+constexpr uint32_t kWholeQuery = 0xffffffffu;
+
 template <int PRED, int W>
 struct TravState {
   typename QueryOps<PRED>::Q q;
@@ -32,6 +35,8 @@ struct TravState {
   uint32_t t;     // tree
   uint32_t L;     // level of the group being visited
   uint32_t g;     // group index at level L
+  uint32_t ceil;  // kWholeQuery, or the top level of a sub-tree taken over from
+                  // another lane (walked alone: no climb above it, no next tree)
 };
 
 // Starts query qid (visiting slot `slot` of the batch) at the top of tree 0.
@@ -49,6 +54,7 @@ __device__ __forceinline__ bool trav_start(const Forest& F, const BatchDesc& B, 
   s.q = QueryOps<PRED>::load(B.queries, s.qid);
   s.ms.clear();
   s.t = 0;
+  s.ceil = kWholeQuery;
   if (F.n_trees == 0) return false;
   const TreeDesc& T = F.tree[0];
   s.L = T.top;
@@ -62,7 +68,8 @@ __device__ __forceinline__ bool trav_start(const Forest& F, const BatchDesc& B, 
 template <int PRED, int W>
 __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>& s) {
   for (;;) {
-    uint32_t top = F.tree[s.t].top;
+    const bool whole = s.ceil == kWholeQuery;
+    uint32_t top = whole ? F.tree[s.t].top : s.ceil;
     while (s.L == 0 || s.ms.get(s.L) == 0) {
       if (s.L == top) break;
       s.L += 1;
@@ -76,6 +83,7 @@ __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>
       s.L -= 1;
       return true;
     }
+    if (!whole) return false;  // a taken-over sub-tree is done
     // This tree is exhausted: enter the next one at its top group.
     s.t += 1;
     if (s.t >= F.n_trees) return false;
@@ -88,12 +96,65 @@ __device__ __forceinline__ bool trav_advance(const Forest& F, TravState<PRED, W>
   }
 }
 
+// Work sharing (warp-collective).  Per-query work is heavily skewed (a query
+// in a dense cluster walks ten times the groups of a typical one), so once a
+// chunk has no unstarted query, lanes whose queries finished would idle until
+// the slowest query of the warp ends.  Instead the k-th idle lane takes over
+// one pending entry of the k-th lane that still has some: the donor clears
+// the highest bit of its mask stack (an entry of its shallowest pending level,
+// the largest sub-tree it has left) and the receiver walks that entry's
+// sub-tree alone (ceil = its top level).  The pairs are the same, found by
+// another lane of the same warp, with the same query id and batch.
+template <int PRED, int W>
+__device__ __forceinline__ void share_work(TravState<PRED, W>& s, bool& active) {
+  const uint32_t idle = __ballot_sync(kFull, !active);
+  if (idle == 0) return;
+  const uint32_t donors = __ballot_sync(kFull, active && s.ms.any());
+  if (donors == 0) return;
+  const uint32_t lane = lane_id();
+  const uint32_t lt = lanemask_lt();
+  const uint32_t k = min(__popc(idle), __popc(donors));
+  uint32_t give_l = 0, give_g = 0;
+  if (((donors >> lane) & 1u) && static_cast<uint32_t>(__popc(donors & lt)) < k) {
+    const uint32_t p = static_cast<uint32_t>(s.ms.pop_highest());
+    const uint32_t lp = p / W + 1;  // level of the pending entry (> s.L)
+    const uint32_t gp = s.g >> (log2_width<W>() * (lp - s.L));  // its group, on this lane's path
+    give_l = lp - 1;
+    give_g = gp * W + (p % W);
+  }
+  const uint32_t irank = __popc(idle & lt);
+  const bool take = !active && irank < k;
+  uint32_t src = lane;
+  if (take) {  // the irank-th donor
+    uint32_t m = donors;
+    for (uint32_t j = 0; j < irank; ++j) m &= m - 1;
+    src = __ffs(m) - 1;
+  }
+  const auto q = shfl_words(s.q, static_cast<int>(src));
+  const uint32_t qid = __shfl_sync(kFull, s.qid, src);
+  const uint32_t rb = __shfl_sync(kFull, s.rb, src);
+  const uint32_t t = __shfl_sync(kFull, s.t, src);
+  const uint32_t gl = __shfl_sync(kFull, give_l, src);
+  const uint32_t gg = __shfl_sync(kFull, give_g, src);
+  if (take) {
+    s.q = q;
+    s.qid = qid;
+    s.rb = rb;
+    s.t = t;
+    s.L = gl;
+    s.g = gg;
+    s.ceil = gl;
+    s.ms.clear();
+    active = true;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // thread scheme
 // ---------------------------------------------------------------------------
 // MODE kUser: H::call<PRED>(geom_id, query_id, arg) once per pair, the
 // reference's per-hit handler contract (ROUTED false).
-template <int PRED, int MODE, int W, bool ROUTED, class H = NoUserHandler>
+template <int PRED, int MODE, int W, bool ROUTED, class H = NoUserHandler, bool SHARE = true>
 __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDesc& B,
                                                  uint32_t cbeg, uint32_t cend, DevPair* wbuf, uint32_t* wbat,
                                                  const uint32_t* only,
@@ -173,13 +234,14 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
         cnt = 0;
       }
     }
-    // Refill finished lanes from the chunk.
+    // Refill finished lanes from the chunk, then share the rest of the work.
     uint32_t idle = __ballot_sync(kFull, !active);
     if (idle != 0 && next < cend) {
       uint32_t slot = next + __popc(idle & lanemask_lt());
       if (!active && slot < cend) active = trav_start<PRED, W, ROUTED>(F, B, slot, s, only, M);
       next = min(cend, next + __popc(idle));
     }
+    if (SHARE && next >= cend) share_work<PRED, W>(s, active);
   }
   if constexpr (MODE == kCollect) out.flush(qu);
   if constexpr (MODE == kCount && !ROUTED)
