@@ -853,7 +853,7 @@ def run_mutable_bench(args, ctx):
     }
 
 
-def serving_check(sv, reqs, boxes, out_buf, grid=None) -> dict:
+def serving_check(sv, reqs, boxes, grid=None) -> dict:
     """Submits `reqs` (closed loop), takes every request's pairs and compares
     each request's count and order-independent pair digest with the oracle
     over `boxes` (query ids 0-based per request)."""
@@ -864,8 +864,9 @@ def serving_check(sv, reqs, boxes, out_buf, grid=None) -> dict:
     tickets = [sv.submit(p, q) for p, q in reqs]
     got = []
     for t in tickets:
-        pr = sv.take(t, out=out_buf)
-        got.append((int(pr.shape[0]), pair_digest(pr)))
+        segs = sv.view(t)
+        got.append((sum(s.shape[0] for s in segs), sum(pair_digest(s) for s in segs) % (1 << 64)))
+        sv.release(t)
     t0 = time.perf_counter()
     own = grid is None
     g = ora.grid_build(boxes, 2.0) if own else grid
@@ -886,6 +887,96 @@ def serving_check(sv, reqs, boxes, out_buf, grid=None) -> dict:
     return {"requests": len(reqs), "pairs": total, "equal": not bad,
             "mismatched_requests": bad[:8], "oracle": "reference" if backend == "ref" else "port",
             "oracle_seconds": time.perf_counter() - t0}
+
+
+def serving_plain_form(ix, reqs, ctx) -> dict:
+    """The plain form of the served mix: each request as one synchronous Query
+    launch through the public API with host buffers (pinned H2D of its
+    queries, the collecting handler into a preallocated queue, D2H of its
+    count and pairs; a request whose pairs overflow the queue runs again with
+    the exact capacity).  Requests run back to back on one stream."""
+    torch = ctx.torch
+    import rtspatial_b200 as rb
+    dev = ctx.dev
+    max_q = max(q.shape[0] for _, q in reqs)
+    q_host = torch.empty(max_q * 4, dtype=torch.float32).pin_memory()
+    q_dev = torch.empty(max_q * 4, dtype=torch.float32, device=dev)
+    cap = 16 << 20
+    qu = rb.Queue(cap, dev)
+    out_host = torch.empty((cap, 2), dtype=torch.int32).pin_memory()
+    stream = torch.cuda.current_stream()
+    lat = []
+    outs = [out_host]
+
+    def one(p, q):
+        n, w = q.shape
+        q_host[:n * w].numpy()[:] = q.reshape(-1)
+        q_dev[:n * w].copy_(q_host[:n * w], non_blocking=True)
+        qd = q_dev[:n * w].view(n, w)
+        for _ in range(2):
+            qu.Clear()
+            ix.Query(p, qd, qu.DeviceObject(), handler=rb.Handler.COLLECT)
+            k = qu.size(stream)
+            if k <= qu.capacity():
+                break
+            qu.Init(k)
+        if k > outs[0].shape[0]:
+            outs[0] = torch.empty((k, 2), dtype=torch.int32).pin_memory()
+        if k:
+            outs[0][:k].copy_(qu.pairs[:k], non_blocking=True)
+        stream.synchronize()
+        return k
+
+    for p, q in reqs[:5]:  # warm-up
+        one(p, q)
+    qu.Init(cap)
+    t_all = time.perf_counter()
+    pairs = 0
+    for p, q in reqs:
+        t0 = time.perf_counter()
+        pairs += one(p, q)
+        lat.append(time.perf_counter() - t0)
+    wall = time.perf_counter() - t_all
+    nq = sum(q.shape[0] for _, q in reqs)
+    lat.sort()
+    return {"value": nq * ctx.world / wall, "unit": "queries/s", "requests": len(reqs),
+            "pairs": pairs, "latency_ms": {"p50": 1000 * lat[len(lat) // 2],
+                                           "p99": 1000 * lat[min(len(lat) - 1,
+                                                                 int(0.99 * (len(lat) - 1)))]},
+            "launches_per_request": 1,
+            "what": "one synchronous Query launch per request, host buffers, requests in "
+                    "sequence (no updates)"}
+
+
+def serving_cpu_rate(boxes, reqs, seconds: float) -> dict:
+    """The CPU reference on the served mix: the oracle's grid (built outside
+    the timing) counts the requests' pairs with every host thread, over as
+    many requests as fit in about `seconds`."""
+    from oracle.oracle import KIND_CONTAINS, KIND_INTERSECTS, KIND_POINT, Oracle
+    import rtspatial_b200 as rb
+    backend = oracle_backend()
+    ora = Oracle(backend)
+    threads = os.cpu_count() or 1
+    g = ora.grid_build(boxes, 2.0)
+    try:
+        n_q, t_used, used = 0, 0.0, 0
+        for p, q in reqs:
+            kind = KIND_POINT if q.shape[1] == 2 else (
+                KIND_INTERSECTS if p == rb.Predicate.kIntersects else KIND_CONTAINS)
+            t0 = time.perf_counter()
+            ora.run_on_grid(g, kind, boxes, np.ascontiguousarray(q), threads)
+            t_used += time.perf_counter() - t0
+            n_q += q.shape[0]
+            used += 1
+            if t_used > seconds:
+                break
+    finally:
+        ora.grid_free(g)
+    return {"value": n_q / t_used, "unit": "queries/s", "cores": threads,
+            "kind": "reference" if backend == "ref" else "port",
+            "sample": f"the first {used} of {len(reqs)} open-loop requests ({n_q} queries) against "
+                      f"the initial {boxes.shape[0]} boxes, uniform-grid filter built outside the "
+                      f"timing, OpenMP, counting only"}
 
 
 def run_serving_bench(args, ctx):
@@ -940,11 +1031,10 @@ def run_serving_bench(args, ctx):
 
     sv = rb.Server(ix, slots=3, max_queries_per_launch=1 << 19, pairs_per_launch=16 << 20,
                    host_result_bytes=4 << 30)
-    # the client's result buffer, reused for every request (touched once here)
-    out_buf = np.ones((64 << 20, 2), dtype=np.uint32)
-
     def take(t):
-        return sv.take(t, out=out_buf)
+        # zero-copy: the pairs are on the host in the server's pinned memory
+        sv.view(t)
+        sv.release(t)
 
     # closed loop: everything submitted at once -> capacity
     warm = make_requests(20)
@@ -961,8 +1051,8 @@ def run_serving_bench(args, ctx):
     total_q = sum(q.shape[0] for _, q in reqs)
     capacity_qps = total_q / closed_s
     parity = {}
-    if check:
-        parity["initial"] = serving_check(sv, reqs, boxes, out_buf)
+    if check:  # every 4th request of the closed loop, run again and checked
+        parity["initial"] = serving_check(sv, reqs[::4], boxes)
     # open loop: Poisson arrivals at 70% of capacity, updates interleaved
     mean_q = total_q / n_req
     lam = 0.7 * capacity_qps / mean_q
@@ -995,6 +1085,10 @@ def run_serving_bench(args, ctx):
     open_s = time.perf_counter() - t0
     clocks_info = clocks.stop()
     st = sv.stats()
+    plain = serving_plain_form(ix, reqs, ctx) if not args.no_plain else None
+    cpu = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu:
+        cpu = serving_cpu_rate(boxes, reqs, args.cpu_seconds)
     if check:
         # the host mirror of the box set after every applied update batch
         final = boxes
@@ -1003,7 +1097,7 @@ def run_serving_bench(args, ctx):
             final[u["delete_ids"], 3] = final[u["delete_ids"], 1]
             final[u["update_ids"]] = u["update_boxes"]
             final = np.concatenate([final, u["inserts"]])
-        parity["final"] = serving_check(sv, make_requests(max(10, n_req // 20)), final, out_buf)
+        parity["final"] = serving_check(sv, make_requests(max(10, n_req // 20)), final)
     sv.close()
     served_q = sum(q.shape[0] for _, q in reqs)
     if parity and not all(v["equal"] for v in parity.values()):
@@ -1028,13 +1122,23 @@ def run_serving_bench(args, ctx):
                         "p99_ms": 1000 * closed["latency_p99_s"],
                         "launches": closed["launches"]},
         "open_loop": {"offered_requests_per_s": lam, "launches": st["launches"],
-                      "pairs": st["pairs_done"], "retried_parts": st["retried_parts"],
-                      "updates": st["updates_done"]},
+                      "parts": st["parts"], "pairs": st["pairs_done"],
+                      "retried_parts": st["retried_parts"], "updates": st["updates_done"]},
+        "stages_s": {"what": "open loop, summed over launches: worker packing, device time of a "
+                             "launch (query copy, sort, kernel, count copy), device copies of "
+                             "pairs to pinned host memory, client take copies, worker applying "
+                             "updates; wall time of the open loop for scale",
+                     "wall": open_s, "pack": st["pack_s"], "launch": st["launch_s"],
+                     "copy_pairs": st["copy_s"], "take": st["take_s"], "update": st["update_s"]},
+        "forms": {"plain": plain},
+        "served_over_plain": (served_q / open_s) / plain["value"] if plain else None,
+        "cpu_baseline": cpu,
         "parity": {"checked": bool(parity), "equal": all(v["equal"] for v in parity.values()),
                    **parity,
-                   "what": "every closed-loop request vs the oracle on the initial boxes; a "
-                           "closed tail after the open loop vs the oracle on the final boxes "
-                           "(per request: pair count and order-independent digest)"},
+                   "what": "every 4th closed-loop request, run again, vs the oracle on the "
+                           "initial boxes; a closed tail after the open loop vs the oracle on "
+                           "the final boxes (per request: pair count and order-independent "
+                           "digest)"},
         "clocks": clocks_info,
     }
 

@@ -317,6 +317,13 @@ typedef struct rts_server_stats {
   uint64_t requests_done, queries_done, pairs_done, launches, retried_parts, updates_done;
   double latency_p50_s, latency_p99_s, latency_max_s; /* submit -> results on the host */
   double elapsed_s;                                   /* first submit -> last completion */
+  /* Where the time went, summed over launches since the last reset: */
+  double pack_s;    /* worker thread: packing parts into pinned staging */
+  double launch_s;  /* device: a launch's query copy, sort, kernel and count copy */
+  double copy_s;    /* device: copies of pairs into the pinned result arena */
+  double take_s;    /* client threads: rts_server_take copying pairs out */
+  double update_s;  /* worker thread: applying update batches (waits for their device work) */
+  uint64_t parts;   /* request parts launched */
 } rts_server_stats;
 int rts_server_config_default(rts_server_config* cfg);
 int rts_server_create(rts_index* index, const rts_server_config* cfg, rts_server** out);
@@ -339,6 +346,16 @@ int rts_server_wait(rts_server* server, uint64_t ticket, double timeout_s);
  * *n_pairs = the first id its inserts received. */
 int rts_server_take(rts_server* server, uint64_t ticket, rts_pair* out, uint64_t capacity,
                     uint64_t* n_pairs);
+/* Zero-copy access to a done query's pairs: the pinned host segments that
+ * hold them, in query order of the request's parts (up to max_segments;
+ * *n_segments gives the number needed, RTS_ERR_QUEUE_FULL when larger), and
+ * their total.  The memory stays valid, and the ticket reserved, until
+ * rts_server_release(ticket). */
+int rts_server_view(rts_server* server, uint64_t ticket, const rts_pair** segments,
+                    uint64_t* segment_pairs, uint32_t max_segments, uint32_t* n_segments,
+                    uint64_t* n_pairs);
+/* Returns a viewed request's pinned memory to the server and forgets it. */
+int rts_server_release(rts_server* server, uint64_t ticket);
 int rts_server_get_stats(rts_server* server, rts_server_stats* stats);
 int rts_server_reset_stats(rts_server* server);
 

@@ -108,7 +108,10 @@ class rts_server_stats(ctypes.Structure):
                 ("pairs_done", ctypes.c_uint64), ("launches", ctypes.c_uint64),
                 ("retried_parts", ctypes.c_uint64), ("updates_done", ctypes.c_uint64),
                 ("latency_p50_s", ctypes.c_double), ("latency_p99_s", ctypes.c_double),
-                ("latency_max_s", ctypes.c_double), ("elapsed_s", ctypes.c_double)]
+                ("latency_max_s", ctypes.c_double), ("elapsed_s", ctypes.c_double),
+                ("pack_s", ctypes.c_double), ("launch_s", ctypes.c_double),
+                ("copy_s", ctypes.c_double), ("take_s", ctypes.c_double),
+                ("update_s", ctypes.c_double), ("parts", ctypes.c_uint64)]
 
 
 class rts_tune_result(ctypes.Structure):
@@ -152,6 +155,9 @@ SIGNATURES = {
     "rts_server_submit_update": (_I, [_P, _P, _U64, _P, _U64, _P, _U64, ctypes.POINTER(_U64)]),
     "rts_server_wait": (_I, [_P, _U64, ctypes.c_double]),
     "rts_server_take": (_I, [_P, _U64, _P, _U64, ctypes.POINTER(_U64)]),
+    "rts_server_view": (_I, [_P, _U64, ctypes.POINTER(_P), ctypes.POINTER(_U64), ctypes.c_uint32,
+                             ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_U64)]),
+    "rts_server_release": (_I, [_P, _U64]),
     "rts_server_get_stats": (_I, [_P, ctypes.POINTER(rts_server_stats)]),
     "rts_server_reset_stats": (_I, [_P]),
     "rts_autotune": (_I, [_P, ctypes.POINTER(rts_batch), ctypes.c_uint32, _I, _P,

@@ -114,6 +114,7 @@ struct Request {
   uint64_t first_new_id = 0;
   int status = RTS_OK;
   bool done = false;
+  bool viewed = false;          // pairs handed out by rts_server_view until release
   double t_submit = 0, t_done = 0;
 };
 
@@ -145,8 +146,10 @@ struct Slot {
   uint32_t max_parts = 0;
   QueryScratch qs;
   cudaEvent_t ev_counts = nullptr, ev_pairs = nullptr, ev_kernel = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_copy0 = nullptr;  // timing: launch start, pair copies start
   std::vector<Part> parts;
   int state = 0;  // 0 free, 1 launched, 2 copying pairs
+  bool overflowed = false;  // state 2: some part must run again with its exact size
   bool waited_update = true;
 };
 
@@ -177,6 +180,8 @@ struct rts_server {
   // statistics
   std::vector<double> lat;
   uint64_t queries_done = 0, pairs_done = 0, launches = 0, retried = 0, updates_done = 0;
+  uint64_t parts = 0;
+  double pack_s = 0, launch_s = 0, copy_s = 0, take_s = 0, update_s = 0;
   double t_first = 0, t_last = 0;
   int fatal = RTS_OK;
 };
@@ -200,8 +205,10 @@ int slot_init(rts_server* sv, Slot& sl, uint64_t in_bytes, uint64_t pairs, uint3
   RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_counts), max_parts * sizeof(uint32_t)));
   RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_queues), max_parts * sizeof(DevQueue)));
   RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.h_descs), max_parts * sizeof(BatchDesc)));
-  RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_counts, cudaEventDisableTiming));
-  RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_pairs, cudaEventDisableTiming));
+  RTS_CUDA_TRY(cudaEventCreate(&sl.ev_counts));
+  RTS_CUDA_TRY(cudaEventCreate(&sl.ev_pairs));
+  RTS_CUDA_TRY(cudaEventCreate(&sl.ev_start));
+  RTS_CUDA_TRY(cudaEventCreate(&sl.ev_copy0));
   RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_kernel, cudaEventDisableTiming));
   if ((rc = buf_reserve(sl.qs.work, sizeof(uint32_t), s, false, 0))) return rc;
   // Order scratch for a full slot (so no launch allocates).
@@ -239,6 +246,8 @@ void slot_free(Slot& sl) {
   if (sl.ev_counts) cudaEventDestroy(sl.ev_counts);
   if (sl.ev_pairs) cudaEventDestroy(sl.ev_pairs);
   if (sl.ev_kernel) cudaEventDestroy(sl.ev_kernel);
+  if (sl.ev_start) cudaEventDestroy(sl.ev_start);
+  if (sl.ev_copy0) cudaEventDestroy(sl.ev_copy0);
   if (s) cudaStreamDestroy(s);
 }
 
@@ -328,6 +337,7 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
     sl.waited_update = true;
   }
   const uint32_t np = static_cast<uint32_t>(sl.parts.size());
+  const double t_pack0 = now_s();
   auto* d_in = static_cast<unsigned char*>(sl.d_in.ptr);
   auto* d_pairs = static_cast<DevPair*>(sl.d_pairs.ptr);
   auto* d_counts = static_cast<uint32_t*>(sl.d_counts.ptr);
@@ -355,8 +365,11 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
     sl.h_descs[i] = d;
   }
   int rc = RTS_OK;
+  sv->pack_s += now_s() - t_pack0;
+  sv->parts += np;
   const bool sorted = want_sort(ix, total);
   if (sorted) rc = plan_order(sl.qs, plan, sl.h_descs, np, total, chunks, s);
+  cudaEventRecord(sl.ev_start, s);
   cudaError_t e = cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, in_used, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(sl.d_queues.ptr, sl.h_queues, np * sizeof(DevQueue), cudaMemcpyHostToDevice, s);
@@ -388,14 +401,18 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
 bool poll_slot(rts_server* sv, Slot& sl) {
   if (sl.state == 1) {
     if (cudaEventQuery(sl.ev_counts) != cudaSuccess) return false;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, sl.ev_start, sl.ev_counts) == cudaSuccess) sv->launch_s += 1e-3 * ms;
     // Reserve arena space for every part that fits its capacity; if the arena
     // is full, try again later (results not yet taken hold it).
     std::vector<size_t> got;
     bool ok = true;
+    sl.overflowed = false;
     for (size_t i = 0; i < sl.parts.size(); ++i) {
       Part& p = sl.parts[i];
       p.count = sl.h_counts[i];
       p.heap = false;
+      sl.overflowed |= p.count > p.cap;
       if (p.count > p.cap || p.count == 0) continue;
       const size_t bytes = p.count * sizeof(rts_pair);
       if (bytes > sv->arena.bytes) {
@@ -414,6 +431,7 @@ bool poll_slot(rts_server* sv, Slot& sl) {
       return false;
     }
     auto* d_pairs = static_cast<rts_pair*>(sl.d_pairs.ptr);
+    cudaEventRecord(sl.ev_copy0, sl.stream);
     for (auto& p : sl.parts) {
       if (p.count > p.cap || p.count == 0 || p.heap) continue;
       cudaMemcpyAsync(sv->arena.base + p.host_off, d_pairs + p.out_off,
@@ -425,6 +443,8 @@ bool poll_slot(rts_server* sv, Slot& sl) {
   }
   if (sl.state == 2) {
     if (cudaEventQuery(sl.ev_pairs) != cudaSuccess) return false;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, sl.ev_copy0, sl.ev_pairs) == cudaSuccess) sv->copy_s += 1e-3 * ms;
     auto* d_pairs = static_cast<rts_pair*>(sl.d_pairs.ptr);
     for (auto& p : sl.parts) {
       Request* r = p.r;
@@ -487,6 +507,7 @@ int stage_and(cudaStream_t us, const void* host, size_t bytes, void** dev) {
 
 void apply_update(rts_server* sv, Request* r) {
   cudaStream_t us = sv->update_stream;
+  const double t0 = now_s();
   int rc = RTS_OK;
   void* d = nullptr;
   if (!r->del.empty()) {
@@ -507,6 +528,7 @@ void apply_update(rts_server* sv, Request* r) {
     if (d) cudaFreeAsync(d, us);
   }
   r->status = rc;
+  sv->update_s += now_s() - t0;
   cudaEventRecord(sv->ev_update, us);
   sv->update_pending_event = true;
   for (auto& sl : sv->slots) sl->waited_update = false;
@@ -527,9 +549,12 @@ void worker_loop(rts_server* sv) {
       finish_request(sv, r);
       progress = true;
     }
-    // An update at the head waits until every earlier query is final.
+    // An update at the head waits until every earlier launch has finished its
+    // kernel and reported its counts (so no part of an earlier query can need
+    // a re-run after it); copies of their pairs may still be in flight, as
+    // they read the launch's own buffers, not the index.
     bool drained = sv->retries.empty();
-    for (auto& sl : sv->slots) drained &= sl->state == 0;
+    for (auto& sl : sv->slots) drained &= sl->state == 0 || (sl->state == 2 && !sl->overflowed);
     if (!sv->pending.empty() && sv->pending.front()->is_update && drained) {
       Request* r = sv->pending.front();
       sv->pending.pop_front();
@@ -730,30 +755,79 @@ int rts_server_wait(rts_server* sv, uint64_t ticket, double timeout_s) {
 int rts_server_take(rts_server* sv, uint64_t ticket, rts_pair* out, uint64_t capacity,
                     uint64_t* n_pairs) {
   if (!sv || !n_pairs) return fail(RTS_ERR_INVALID_ARGUMENT, "server or n_pairs is null");
+  std::unique_ptr<Request> owned;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    auto it = sv->reqs.find(ticket);
+    if (it == sv->reqs.end()) return fail(RTS_ERR_INVALID_ARGUMENT, "unknown ticket");
+    Request* r = it->second.get();
+    if (!r->done) return fail(RTS_ERR_INVALID_ARGUMENT, "request not done");
+    if (r->viewed) return fail(RTS_ERR_INVALID_ARGUMENT, "request is viewed: release it");
+    *n_pairs = r->is_update ? r->first_new_id : r->n_out;
+    if (r->is_update) {
+      int st = r->status;
+      sv->reqs.erase(it);
+      return st;
+    }
+    if (capacity < r->n_out || (!out && r->n_out))
+      return fail(RTS_ERR_QUEUE_FULL, "output capacity smaller than the result");
+    owned = std::move(it->second);  // off the ticket table: its arena chunks stay reserved
+    sv->reqs.erase(it);
+  }
+  // The copy runs without the server lock, so the worker keeps launching.
+  const double t0 = now_s();
+  uint64_t at = 0;
+  for (auto& c : owned->out) {
+    const rts_pair* src = (c.off == ~size_t(0))
+                              ? c.heap.data()
+                              : reinterpret_cast<const rts_pair*>(sv->arena.base + c.off);
+    std::memcpy(out + at, src, c.n * sizeof(rts_pair));
+    at += c.n;
+  }
+  std::lock_guard<std::mutex> lock(sv->mu);
+  sv->take_s += now_s() - t0;
+  release_chunks(sv, owned.get());
+  return owned->status;
+}
+
+int rts_server_view(rts_server* sv, uint64_t ticket, const rts_pair** segments,
+                    uint64_t* segment_pairs, uint32_t max_segments, uint32_t* n_segments,
+                    uint64_t* n_pairs) {
+  if (!sv || !n_segments || !n_pairs)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "server, n_segments or n_pairs is null");
   std::lock_guard<std::mutex> lock(sv->mu);
   auto it = sv->reqs.find(ticket);
   if (it == sv->reqs.end()) return fail(RTS_ERR_INVALID_ARGUMENT, "unknown ticket");
   Request* r = it->second.get();
   if (!r->done) return fail(RTS_ERR_INVALID_ARGUMENT, "request not done");
-  *n_pairs = r->is_update ? r->first_new_id : r->n_out;
-  if (r->is_update) {
-    int st = r->status;
-    sv->reqs.erase(it);
-    return st;
+  if (r->is_update) return fail(RTS_ERR_INVALID_ARGUMENT, "an update ticket has no pairs");
+  *n_pairs = r->n_out;
+  *n_segments = static_cast<uint32_t>(r->out.size());
+  if (r->out.size() > max_segments)
+    return fail(RTS_ERR_QUEUE_FULL, "more segments than max_segments");
+  if (!r->out.empty() && (!segments || !segment_pairs))
+    return fail(RTS_ERR_INVALID_ARGUMENT, "segments or segment_pairs is null");
+  for (size_t i = 0; i < r->out.size(); ++i) {
+    const Chunk& c = r->out[i];
+    segments[i] = (c.off == ~size_t(0))
+                      ? c.heap.data()
+                      : reinterpret_cast<const rts_pair*>(sv->arena.base + c.off);
+    segment_pairs[i] = c.n;
   }
-  if (capacity < r->n_out || (!out && r->n_out))
-    return fail(RTS_ERR_QUEUE_FULL, "output capacity smaller than the result");
-  uint64_t at = 0;
-  for (auto& c : r->out) {
-    const rts_pair* src = (c.off == ~size_t(0)) ? c.heap.data()
-                                                : reinterpret_cast<const rts_pair*>(sv->arena.base + c.off);
-    std::memcpy(out + at, src, c.n * sizeof(rts_pair));
-    at += c.n;
-  }
+  r->viewed = true;
+  return r->status;
+}
+
+int rts_server_release(rts_server* sv, uint64_t ticket) {
+  if (!sv) return fail(RTS_ERR_INVALID_ARGUMENT, "server is null");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return fail(RTS_ERR_INVALID_ARGUMENT, "unknown ticket");
+  Request* r = it->second.get();
+  if (!r->done) return fail(RTS_ERR_INVALID_ARGUMENT, "request not done");
   release_chunks(sv, r);
-  int st = r->status;
   sv->reqs.erase(it);
-  return st;
+  return RTS_OK;
 }
 
 int rts_server_get_stats(rts_server* sv, rts_server_stats* st) {
@@ -777,6 +851,12 @@ int rts_server_get_stats(rts_server* sv, rts_server_stats* st) {
   st->latency_p99_s = pct(0.99);
   st->latency_max_s = l.empty() ? 0.0 : l.back();
   st->elapsed_s = (sv->t_last > sv->t_first) ? sv->t_last - sv->t_first : 0.0;
+  st->pack_s = sv->pack_s;
+  st->launch_s = sv->launch_s;
+  st->copy_s = sv->copy_s;
+  st->take_s = sv->take_s;
+  st->update_s = sv->update_s;
+  st->parts = sv->parts;
   return RTS_OK;
 }
 
@@ -785,6 +865,8 @@ int rts_server_reset_stats(rts_server* sv) {
   std::lock_guard<std::mutex> lock(sv->mu);
   sv->lat.clear();
   sv->queries_done = sv->pairs_done = sv->launches = sv->retried = sv->updates_done = 0;
+  sv->parts = 0;
+  sv->pack_s = sv->launch_s = sv->copy_s = sv->take_s = sv->update_s = 0;
   sv->t_first = sv->t_last = 0;
   return RTS_OK;
 }

@@ -79,6 +79,35 @@ class Server:
         check(lib().rts_server_take(self._h, ticket, out.ctypes.data, n.value, ctypes.byref(n)))
         return out[:n.value]
 
+    def view(self, ticket: int) -> list:
+        """Zero-copy: the request's pairs as (k, 2) uint32 numpy arrays over the
+        server's pinned result memory, one per part in query order (waits for
+        the request).  Valid until ``release(ticket)``."""
+        self.wait(ticket)
+        n_seg = ctypes.c_uint32()
+        n = ctypes.c_uint64()
+        cap = 64
+        while True:
+            segs = (ctypes.c_void_p * cap)()
+            cnts = (ctypes.c_uint64 * cap)()
+            rc = lib().rts_server_view(self._h, ticket, segs, cnts, cap, ctypes.byref(n_seg),
+                                       ctypes.byref(n))
+            if rc == L.RTS_ERR_QUEUE_FULL and n_seg.value > cap:
+                cap = n_seg.value
+                continue
+            check(rc)
+            break
+        out = []
+        for i in range(n_seg.value):
+            k = int(cnts[i])
+            buf = (ctypes.c_uint32 * (2 * k)).from_address(segs[i])
+            out.append(np.frombuffer(buf, dtype=np.uint32).reshape(k, 2))
+        return out
+
+    def release(self, ticket: int) -> None:
+        """Ends a ``view``: the pinned memory returns to the server."""
+        check(lib().rts_server_release(self._h, ticket))
+
     def stats(self) -> dict:
         st = L.rts_server_stats()
         check(lib().rts_server_get_stats(self._h, ctypes.byref(st)))

@@ -106,3 +106,29 @@ def test_server_overflow_reruns_exactly(cuda, oracle):
     assert st["retried_parts"] > 0
     for (k, q), g in zip(reqs, got):
         assert_same_pairs(g, oracle.run(KIND[k][0], boxes, q)[2], "after re-runs")
+
+
+def test_server_zero_copy_views_and_stage_times(cuda, oracle):
+    """rts_server_view hands out the pinned segments of a request's pairs
+    without a copy; after release the memory serves later requests; the
+    per-stage times of the statistics add up to something positive."""
+    rng = np.random.default_rng(33)
+    boxes = wl.uniform_boxes(rng, 80_000, 1e-2)
+    ix = rb.SpatialIndex(rb.Config())
+    ix.Insert(dev(boxes))
+    torch.cuda.synchronize()
+    # a small result arena: released views must make room for later requests
+    sv = rb.Server(ix, slots=2, max_queries_per_launch=16 * 1024, pairs_per_launch=1 << 20,
+                   host_result_bytes=8 << 20)
+    for rnd in range(3):
+        reqs = make_requests(rng, 12, max_n=8000)
+        tickets = [sv.submit(KIND[k][1], q) for k, q in reqs]
+        for (k, q), t in zip(reqs, tickets):
+            segs = sv.view(t)
+            got = np.concatenate(segs) if segs else np.zeros((0, 2), np.uint32)
+            assert_same_pairs(canon(got), oracle.run(KIND[k][0], boxes, q)[2], f"round {rnd}")
+            sv.release(t)
+    st = sv.stats()
+    sv.close()
+    assert st["parts"] >= st["launches"] > 0
+    assert st["launch_s"] > 0 and st["copy_s"] > 0 and st["pack_s"] > 0
