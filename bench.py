@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--sort", type=int, default=-1, help="sort_queries: 0 never, 1 always, 2 auto")
     ap.add_argument("--occupancy", type=int, default=-1)
+    ap.add_argument("--group-loads", type=int, default=-1,
+                    help="L1 use of the group loads: 0 auto, 1 cached, 2 streaming")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-others", action="store_true",
                     help="default run only: skip the reduced runs of configs 1, 3, 4, 5")
@@ -82,6 +84,8 @@ def parse():
     ap.add_argument("--rounds", type=int, default=0,
                     help="config 4: mutation rounds (default 50, the configuration's)")
     ap.add_argument("--requests", type=int, default=600, help="config 5: requests per run")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="config 5: the server issues its launches directly (no graph replay)")
     return ap.parse_args()
 
 
@@ -367,7 +371,7 @@ def make_index(args, rb):
         if v:
             setattr(cfg, k, v)
     for k, v in (("traversal", args.traversal), ("curve", args.curve), ("sort_queries", args.sort),
-                 ("query_occupancy", args.occupancy)):
+                 ("query_occupancy", args.occupancy), ("group_loads", args.group_loads)):
         if v >= 0:
             setattr(cfg, k, v)
     return rb.SpatialIndex(cfg)
@@ -642,6 +646,7 @@ def run_query_bench(args, ctx):
                 "node_width": ix.config.node_width, "traversal": ix.config.traversal,
                 "curve": ix.config.curve, "sort_queries": ix.config.sort_queries,
                 "query_occupancy": ix.config.query_occupancy, "chunk": ix.config.chunk,
+                "group_loads": ix.config.group_loads,
                 "l2": "index > L2 and L2 flushed before every timed step (256 MiB write "
                       "outside the events)",
             },
@@ -1030,7 +1035,7 @@ def run_serving_bench(args, ctx):
         return u
 
     sv = rb.Server(ix, slots=3, max_queries_per_launch=1 << 19, pairs_per_launch=16 << 20,
-                   host_result_bytes=4 << 30)
+                   host_result_bytes=4 << 30, use_graphs=not args.no_graphs)
     def take(t):
         # zero-copy: the pairs are on the host in the server's pinned memory
         sv.view(t)
@@ -1113,7 +1118,8 @@ def run_serving_bench(args, ctx):
                                f"{n_req} requests, sizes log-uniform [1,100K], 50% point / "
                                f"25% contains / 25% intersects, Poisson arrivals at 70% of "
                                f"closed-loop capacity, update batches of 0.1% every 10 requests",
-                   "slots": 3},
+                   "slots": 3,
+                   "launches": "CUDA-graph replay per slot" if not args.no_graphs else "direct"},
         "latency_ms": {"p50": 1000 * st["latency_p50_s"], "p99": 1000 * st["latency_p99_s"],
                        "max": 1000 * st["latency_max_s"],
                        "what": "request submit -> its pairs on the host"},
@@ -1128,8 +1134,10 @@ def run_serving_bench(args, ctx):
                              "launch (query copy, sort, kernel, count copy), device copies of "
                              "pairs to pinned host memory, client take copies, worker applying "
                              "updates; wall time of the open loop for scale",
-                     "wall": open_s, "pack": st["pack_s"], "launch": st["launch_s"],
-                     "copy_pairs": st["copy_s"], "take": st["take_s"], "update": st["update_s"]},
+                     "wall": open_s, "pack": st["pack_s"], "issue": st["issue_s"],
+                     "launch": st["launch_s"], "copy_pairs": st["copy_s"], "take": st["take_s"],
+                     "update": st["update_s"]},
+        "graph_launches": st["graph_launches"],
         "forms": {"plain": plain},
         "served_over_plain": (served_q / open_s) / plain["value"] if plain else None,
         "cpu_baseline": cpu,

@@ -72,6 +72,7 @@ struct Config {
   int sort_queries = 2;
   int query_occupancy = 0;
   float frontier_factor = 0.0f;
+  int group_loads = RTS_LOADS_AUTO;
 };
 
 template <typename COORD_T, int N_DIMS>
@@ -119,6 +120,7 @@ class SpatialIndex {
     c.sort_queries = config.sort_queries;
     c.query_occupancy = config.query_occupancy;
     c.frontier_factor = config.frontier_factor;
+    c.group_loads = config.group_loads;
     c.coord_bits = kF64 ? 64 : 32;
     if (h_) rts_destroy(h_);
     h_ = nullptr;

@@ -137,8 +137,14 @@ typedef struct rts_config {
                               (queries beyond it are answered depth-first); 0 = 16 */
   int32_t coord_bits;      /* 32: SpatialIndex<float, 2>; 64: SpatialIndex<double, 2>, whose
                               envelopes, points and updates go through the _f64 calls */
-  int32_t reserved;
+  int32_t group_loads;     /* RTS_LOADS_*: how the thread scheme's node-group loads use L1 */
 } rts_config;
+
+#define RTS_LOADS_AUTO 0      /* streaming for collecting (and user-handler) launches once the
+                                 stored envelopes pass 64 MB; cached otherwise */
+#define RTS_LOADS_CACHED 1    /* groups are cached in L1 (small, hot trees) */
+#define RTS_LOADS_STREAMING 2 /* groups bypass L1 allocation (L1::no_allocate) and fetch whole
+                                 256-byte L2 lines: L1 keeps the kernel's own working set */
 
 #define RTS_TRAVERSAL_AUTO 0   /* packet for range-intersects launches, thread otherwise */
 #define RTS_TRAVERSAL_THREAD 1 /* one thread per query, loops over a node's children */
@@ -285,7 +291,7 @@ typedef struct rts_tune_result {
   int32_t node_width, traversal, query_occupancy, sort_queries;
   uint32_t chunk, candidates;
   int32_t collecting; /* 1: timed with the collecting handler, 0: counting (huge results) */
-  int32_t reserved;
+  int32_t group_loads; /* RTS_LOADS_CACHED or RTS_LOADS_STREAMING, as kept */
   double best_ms;     /* median launch time of the kept settings */
   double first_ms;    /* median launch time of the first candidate */
 } rts_tune_result;
@@ -312,6 +318,10 @@ typedef struct rts_server_config {
   uint64_t pairs_per_launch;       /* pair capacity of one launch arena */
   uint64_t hbm_budget_bytes;       /* bound on all arenas (0 = half the free HBM) */
   uint64_t host_result_bytes;      /* pinned host memory holding results until taken */
+  uint32_t use_graphs;             /* 1 (default): each launch replays its slot's CUDA graph of
+                                      the sequence (input copies, order sort, kernel, count copy),
+                                      updated in place; 0: direct launches */
+  uint32_t reserved;
 } rts_server_config;
 typedef struct rts_server_stats {
   uint64_t requests_done, queries_done, pairs_done, launches, retried_parts, updates_done;
@@ -324,6 +334,8 @@ typedef struct rts_server_stats {
   double take_s;    /* client threads: rts_server_take copying pairs out */
   double update_s;  /* worker thread: applying update batches (waits for their device work) */
   uint64_t parts;   /* request parts launched */
+  uint64_t graph_launches;  /* launches that replayed their slot's CUDA graph */
+  double issue_s;   /* worker thread: issuing launches (API calls, or capture + update + replay) */
 } rts_server_stats;
 int rts_server_config_default(rts_server_config* cfg);
 int rts_server_create(rts_index* index, const rts_server_config* cfg, rts_server** out);

@@ -32,6 +32,9 @@ RTS_TRAVERSAL_TEAM = 2
 RTS_TRAVERSAL_FRONTIER = 3
 RTS_TRAVERSAL_PACKET = 4
 RTS_TRAVERSAL_STAGED = 5
+RTS_LOADS_AUTO = 0
+RTS_LOADS_CACHED = 1
+RTS_LOADS_STREAMING = 2
 RTS_STATUS_WAIT_TIMEOUT = 1
 RTS_CURVE_MORTON = 0
 RTS_CURVE_HILBERT = 1
@@ -67,7 +70,7 @@ class rts_config(ctypes.Structure):
         ("query_occupancy", ctypes.c_int32),
         ("frontier_factor", ctypes.c_float),
         ("coord_bits", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("group_loads", ctypes.c_int32),
     ]
 
 
@@ -100,7 +103,8 @@ class rts_batch(ctypes.Structure):
 class rts_server_config(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("max_parts_per_launch", ctypes.c_uint32),
                 ("max_queries_per_launch", ctypes.c_uint64), ("pairs_per_launch", ctypes.c_uint64),
-                ("hbm_budget_bytes", ctypes.c_uint64), ("host_result_bytes", ctypes.c_uint64)]
+                ("hbm_budget_bytes", ctypes.c_uint64), ("host_result_bytes", ctypes.c_uint64),
+                ("use_graphs", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class rts_server_stats(ctypes.Structure):
@@ -111,14 +115,15 @@ class rts_server_stats(ctypes.Structure):
                 ("latency_max_s", ctypes.c_double), ("elapsed_s", ctypes.c_double),
                 ("pack_s", ctypes.c_double), ("launch_s", ctypes.c_double),
                 ("copy_s", ctypes.c_double), ("take_s", ctypes.c_double),
-                ("update_s", ctypes.c_double), ("parts", ctypes.c_uint64)]
+                ("update_s", ctypes.c_double), ("parts", ctypes.c_uint64),
+                ("graph_launches", ctypes.c_uint64), ("issue_s", ctypes.c_double)]
 
 
 class rts_tune_result(ctypes.Structure):
     _fields_ = [("node_width", ctypes.c_int32), ("traversal", ctypes.c_int32),
                 ("query_occupancy", ctypes.c_int32), ("sort_queries", ctypes.c_int32),
                 ("chunk", ctypes.c_uint32), ("candidates", ctypes.c_uint32),
-                ("collecting", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("collecting", ctypes.c_int32), ("group_loads", ctypes.c_int32),
                 ("best_ms", ctypes.c_double), ("first_ms", ctypes.c_double)]
 
 

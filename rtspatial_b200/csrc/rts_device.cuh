@@ -128,6 +128,25 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uin
 constexpr uint32_t kWaitSpinLimit = 1u << 22;
 constexpr uint32_t kErrWaitTimeout = 1u;
 
+// ldg_box_pair for streaming group loads: no L1 allocation (groups of a large
+// index are rarely reused before eviction and would push out the kernel's
+// own working set) and a 256-byte L2 fetch on a miss (a W16 group is two
+// 128-byte lines, 256-byte aligned).
+__device__ __forceinline__ void ldg_box_pair_stream(const float4* p, float4& a, float4& b) {
+  unsigned long long x0, x1, x2, x3;
+  asm("ld.global.nc.L1::no_allocate.L2::256B.v4.b64 {%0, %1, %2, %3}, [%4];"
+      : "=l"(x0), "=l"(x1), "=l"(x2), "=l"(x3)
+      : "l"(p));
+  a = make_float4(__uint_as_float(static_cast<uint32_t>(x0)),
+                  __uint_as_float(static_cast<uint32_t>(x0 >> 32)),
+                  __uint_as_float(static_cast<uint32_t>(x1)),
+                  __uint_as_float(static_cast<uint32_t>(x1 >> 32)));
+  b = make_float4(__uint_as_float(static_cast<uint32_t>(x2)),
+                  __uint_as_float(static_cast<uint32_t>(x2 >> 32)),
+                  __uint_as_float(static_cast<uint32_t>(x3)),
+                  __uint_as_float(static_cast<uint32_t>(x3 >> 32)));
+}
+
 struct TreeDesc {
   const float4* leaves;  // first slot of this tree
   const DBox* leaves64;  // double index: the double envelopes of the same slots
@@ -145,6 +164,9 @@ struct Forest {
   uint32_t* err;             // device status word of the index (kErr* bits), or nullptr
   uint32_t n_trees;
   uint32_t width;
+  // thread scheme: group loads bypass L1 allocation, for launches that
+  // collect (or call user handlers) and for launches that count
+  uint32_t stream_collect, stream_count;
 };
 
 // Collecting handler target: member layout of

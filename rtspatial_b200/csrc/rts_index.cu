@@ -304,6 +304,20 @@ static int merge_small_trees(rts_index* ix, cudaStream_t s) {
   return RTS_OK;
 }
 
+// Whether the thread scheme's group loads bypass L1 allocation: as asked, or
+// (auto) for collecting launches once the stored envelopes pass 64 MB.  A
+// collecting launch stages its pairs through registers that spill to local
+// memory, and L1 is better spent on those spills than on groups of a large
+// index that are rarely reused; a counting launch spills less.  Measured on
+// B200: streaming took config 2 (collecting, 10M boxes, 160 MB) from 1.56 to
+// 1.37 ms, but config 1 (1M boxes, 16 MB, a tree hot in L1) from 0.061 to
+// 0.075 ms and config 4's counting rounds (20M boxes) from 1.80 to 2.22 ms.
+bool group_loads_streaming(const rts_index* ix, bool collecting) {
+  if (ix->cfg.group_loads == RTS_LOADS_STREAMING) return true;
+  if (ix->cfg.group_loads == RTS_LOADS_CACHED) return false;
+  return collecting && ix->slot_end * sizeof(float4) > (64ull << 20);
+}
+
 int refresh_forest(rts_index* ix) {
   if (!ix->forest_dirty) return RTS_OK;
   // The thread scheme reads a W-group as W / 2 32-byte loads: the buffers the
@@ -319,6 +333,8 @@ int refresh_forest(rts_index* ix) {
   F.width = static_cast<uint32_t>(ix->W);
   F.ids_base = ids_of(ix);
   F.err = static_cast<uint32_t*>(ix->status.ptr);
+  F.stream_collect = group_loads_streaming(ix, true) ? 1u : 0u;
+  F.stream_count = group_loads_streaming(ix, false) ? 1u : 0u;
   for (size_t i = 0; i < ix->trees.size(); ++i) {
     const HostTree& h = ix->trees[i];
     TreeDesc& d = F.tree[i];
@@ -697,6 +713,8 @@ int rts_create(const rts_config* cfg, rts_index** out) {
     return fail(RTS_ERR_INVALID_ARGUMENT, "bad curve");
   if (c.max_trees < 1 || c.max_trees > kMaxTrees)
     return fail(RTS_ERR_INVALID_ARGUMENT, "max_trees must be in 1..16");
+  if (c.group_loads < RTS_LOADS_AUTO || c.group_loads > RTS_LOADS_STREAMING)
+    return fail(RTS_ERR_INVALID_ARGUMENT, "bad group_loads");
   if (c.coord_bits == 0) c.coord_bits = 32;
   if (c.coord_bits != 32 && c.coord_bits != 64)
     return fail(RTS_ERR_INVALID_ARGUMENT, "coord_bits must be 32 or 64");

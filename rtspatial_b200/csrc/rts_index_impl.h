@@ -129,6 +129,7 @@ inline DBox* leaves64_of(rts_index* ix) {
 }
 
 int refresh_forest(rts_index* ix);
+bool group_loads_streaming(const rts_index* ix, bool collecting);
 // Re-sorts every box of the index into one tree at the index's node width.
 int rebuild_all(rts_index* ix, cudaStream_t s);
 LaunchPlan plan_for(const rts_index* ix, int pred, uint64_t total_queries);

@@ -145,8 +145,9 @@ struct Slot {
   uint64_t in_cap = 0, pair_cap = 0;
   uint32_t max_parts = 0;
   QueryScratch qs;
-  cudaEvent_t ev_counts = nullptr, ev_pairs = nullptr, ev_kernel = nullptr;
+  cudaEvent_t ev_counts = nullptr, ev_pairs = nullptr;
   cudaEvent_t ev_start = nullptr, ev_copy0 = nullptr;  // timing: launch start, pair copies start
+  cudaGraphExec_t gexec = nullptr;  // replayed launch sequence of an unsorted launch
   std::vector<Part> parts;
   int state = 0;  // 0 free, 1 launched, 2 copying pairs
   bool overflowed = false;  // state 2: some part must run again with its exact size
@@ -180,8 +181,8 @@ struct rts_server {
   // statistics
   std::vector<double> lat;
   uint64_t queries_done = 0, pairs_done = 0, launches = 0, retried = 0, updates_done = 0;
-  uint64_t parts = 0;
-  double pack_s = 0, launch_s = 0, copy_s = 0, take_s = 0, update_s = 0;
+  uint64_t parts = 0, graph_launches = 0;
+  double pack_s = 0, launch_s = 0, copy_s = 0, take_s = 0, update_s = 0, issue_s = 0;
   double t_first = 0, t_last = 0;
   int fatal = RTS_OK;
 };
@@ -209,7 +210,6 @@ int slot_init(rts_server* sv, Slot& sl, uint64_t in_bytes, uint64_t pairs, uint3
   RTS_CUDA_TRY(cudaEventCreate(&sl.ev_pairs));
   RTS_CUDA_TRY(cudaEventCreate(&sl.ev_start));
   RTS_CUDA_TRY(cudaEventCreate(&sl.ev_copy0));
-  RTS_CUDA_TRY(cudaEventCreateWithFlags(&sl.ev_kernel, cudaEventDisableTiming));
   if ((rc = buf_reserve(sl.qs.work, sizeof(uint32_t), s, false, 0))) return rc;
   // Order scratch for a full slot (so no launch allocates).
   const uint64_t maxq = in_bytes / (2 * sizeof(float));
@@ -245,7 +245,7 @@ void slot_free(Slot& sl) {
   if (sl.h_descs) cudaFreeHost(sl.h_descs);
   if (sl.ev_counts) cudaEventDestroy(sl.ev_counts);
   if (sl.ev_pairs) cudaEventDestroy(sl.ev_pairs);
-  if (sl.ev_kernel) cudaEventDestroy(sl.ev_kernel);
+  if (sl.gexec) cudaGraphExecDestroy(sl.gexec);
   if (sl.ev_start) cudaEventDestroy(sl.ev_start);
   if (sl.ev_copy0) cudaEventDestroy(sl.ev_copy0);
   if (s) cudaStreamDestroy(s);
@@ -367,30 +367,79 @@ bool admit_and_launch(rts_server* sv, Slot& sl) {
   int rc = RTS_OK;
   sv->pack_s += now_s() - t_pack0;
   sv->parts += np;
+  const double t_issue0 = now_s();
   const bool sorted = want_sort(ix, total);
   if (sorted) rc = plan_order(sl.qs, plan, sl.h_descs, np, total, chunks, s);
-  cudaEventRecord(sl.ev_start, s);
-  cudaError_t e = cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, in_used, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(sl.d_queues.ptr, sl.h_queues, np * sizeof(DevQueue), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(sl.d_descs.ptr, sl.h_descs, np * sizeof(BatchDesc), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_counts, 0, np * sizeof(uint32_t), s);
-  if (e != cudaSuccess) rc = cuda_fail(e, "server launch staging");
   if (!rc) rc = refresh_forest(ix);
+  if (!rc) rc = prepare_query_kernel(plan);  // outside any capture
+  cudaEventRecord(sl.ev_start, s);
   const BatchDesc* dd = static_cast<const BatchDesc*>(sl.d_descs.ptr);
-  if (!rc && sorted)
-    rc = fill_order(ix, sl.qs, plan, sl.h_descs, np > 1 ? dd : nullptr, np, total, chunks, s);
-  if (!rc)
-    rc = launch_queries(ix->forest, plan, sl.h_descs, np > 1 ? dd : nullptr, np,
-                        static_cast<uint32_t>(chunks), static_cast<uint32_t*>(sl.qs.work.ptr), s);
-  if (!rc) {
-    e = cudaEventRecord(sl.ev_kernel, s);
+  // The launch sequence: inputs in, counters cleared, (visiting order,) the
+  // persistent kernel, counts out.
+  auto issue = [&]() -> int {
+    cudaError_t e = cudaMemcpyAsync(sl.d_in.ptr, sl.h_in, in_used, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sl.d_queues.ptr, sl.h_queues, np * sizeof(DevQueue),
+                          cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sl.d_descs.ptr, sl.h_descs, np * sizeof(BatchDesc),
+                          cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_counts, 0, np * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "server launch staging");
+    int r = RTS_OK;
+    if (sorted)
+      r = fill_order(ix, sl.qs, plan, sl.h_descs, np > 1 ? dd : nullptr, np, total, chunks, s);
+    if (!r)
+      r = launch_queries(ix->forest, plan, sl.h_descs, np > 1 ? dd : nullptr, np,
+                         static_cast<uint32_t>(chunks), static_cast<uint32_t*>(sl.qs.work.ptr), s);
+    if (!r) {
       e = cudaMemcpyAsync(sl.h_counts, d_counts, np * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaEventRecord(sl.ev_counts, s);
+      if (e != cudaSuccess) r = cuda_fail(e, "server launch");
+    }
+    return r;
+  };
+  if (!rc && sv->cfg.use_graphs) {
+    // CUDA-graph replay: the slot keeps one executable graph of the sequence;
+    // each launch records the sequence with its own sizes and arguments and
+    // updates the executable graph in place (re-instantiating it only when the
+    // sequence's shape changed, e.g. a sort of another number of passes),
+    // then replays it.
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) rc = cuda_fail(e, "server graph capture");
+    if (!rc) {
+      const int r = issue();
+      e = cudaStreamEndCapture(s, &g);
+      rc = r ? r : (e != cudaSuccess ? cuda_fail(e, "server graph capture") : RTS_OK);
+    }
+    if (!rc) {
+      bool fresh = !sl.gexec;
+      if (!fresh) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(sl.gexec, g, &info) != cudaSuccess) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(sl.gexec);
+          sl.gexec = nullptr;
+          fresh = true;
+        }
+      }
+      if (fresh && (e = cudaGraphInstantiate(&sl.gexec, g, 0)) != cudaSuccess) {
+        sl.gexec = nullptr;
+        rc = cuda_fail(e, "server graph instantiate");
+      }
+      if (!rc && (e = cudaGraphLaunch(sl.gexec, s)) != cudaSuccess)
+        rc = cuda_fail(e, "server graph launch");
+      if (!rc) sv->graph_launches++;
+    }
+    if (g) cudaGraphDestroy(g);
+  } else if (!rc) {
+    rc = issue();
+  }
+  if (!rc) {
+    cudaError_t e = cudaEventRecord(sl.ev_counts, s);
     if (e != cudaSuccess) rc = cuda_fail(e, "server launch");
   }
+  sv->issue_s += now_s() - t_issue0;
   if (rc) sv->fatal = rc;
   sl.state = 1;
   sv->launches++;
@@ -594,6 +643,7 @@ int rts_server_config_default(rts_server_config* c) {
   c->pairs_per_launch = 32ull << 20;
   c->hbm_budget_bytes = 0;
   c->host_result_bytes = 1ull << 30;
+  c->use_graphs = 1;
   return RTS_OK;
 }
 
@@ -857,6 +907,8 @@ int rts_server_get_stats(rts_server* sv, rts_server_stats* st) {
   st->take_s = sv->take_s;
   st->update_s = sv->update_s;
   st->parts = sv->parts;
+  st->graph_launches = sv->graph_launches;
+  st->issue_s = sv->issue_s;
   return RTS_OK;
 }
 
@@ -865,8 +917,8 @@ int rts_server_reset_stats(rts_server* sv) {
   std::lock_guard<std::mutex> lock(sv->mu);
   sv->lat.clear();
   sv->queries_done = sv->pairs_done = sv->launches = sv->retried = sv->updates_done = 0;
-  sv->parts = 0;
-  sv->pack_s = sv->launch_s = sv->copy_s = sv->take_s = sv->update_s = 0;
+  sv->parts = sv->graph_launches = 0;
+  sv->pack_s = sv->launch_s = sv->copy_s = sv->take_s = sv->update_s = sv->issue_s = 0;
   sv->t_first = sv->t_last = 0;
   return RTS_OK;
 }

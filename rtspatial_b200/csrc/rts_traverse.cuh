@@ -194,8 +194,13 @@ __device__ __forceinline__ void run_chunk_thread(const Forest& F, const BatchDes
       const float4* p = at_leaf ? T.leaves + first : T.nodes + T.level_off[s.L] + first;
       const uint32_t lim = (at_leaf ? T.n : T.level_cnt[s.L]) - first;
       float4 e[W];
+      if (MODE == kCount ? F.stream_count : F.stream_collect) {  // the same for every lane
 #pragma unroll
-      for (int c = 0; c < W; c += 2) ldg_box_pair(p + c, e[c], e[c + 1]);
+        for (int c = 0; c < W; c += 2) ldg_box_pair_stream(p + c, e[c], e[c + 1]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < W; c += 2) ldg_box_pair(p + c, e[c], e[c + 1]);
+      }
       uint32_t m = 0;
 #pragma unroll
       for (int c = 0; c < W; ++c)

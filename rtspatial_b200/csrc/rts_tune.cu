@@ -172,7 +172,8 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
     }
     if (rc) break;
   }
-  // 4. Keep the winner.
+  // 4. Keep the winner; for the thread scheme, also its L1 policy of the
+  //    group loads (cached or streaming), timed both ways.
   ix->cfg = saved;
   if (!rc) {
     ix->cfg.traversal = best_c.traversal;
@@ -182,6 +183,22 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
     rc = rebuild_at_width(ix, best_w, s);
   } else {
     rebuild_at_width(ix, saved.node_width, s);
+  }
+  if (!rc && best_c.traversal == RTS_TRAVERSAL_THREAD) {
+    double pol_ms[2] = {0, 0};
+    const int pol[2] = {RTS_LOADS_CACHED, RTS_LOADS_STREAMING};
+    for (int i = 0; i < 2 && !rc; ++i) {
+      ix->cfg.group_loads = pol[i];
+      ix->forest_dirty = true;
+      rc = time_launches(ix, b, 3, s, qsize, n_batches, &pol_ms[i]);
+      ++tried;
+    }
+    if (!rc) {
+      const int k = pol_ms[1] < pol_ms[0] ? 1 : 0;
+      ix->cfg.group_loads = pol[k];
+      best = std::min(best, pol_ms[k]);
+    }
+    ix->forest_dirty = true;
   }
   cleanup();
   if (rc) return rc;
@@ -194,5 +211,6 @@ extern "C" int rts_autotune(rts_index* ix, const rts_batch* batches, uint32_t n_
   out->best_ms = best;
   out->first_ms = first;
   out->collecting = collect ? 1 : 0;
+  out->group_loads = group_loads_streaming(ix, collect) ? RTS_LOADS_STREAMING : RTS_LOADS_CACHED;
   return RTS_OK;
 }

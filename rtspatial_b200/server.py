@@ -14,7 +14,8 @@ from ._lib import check, lib
 class Server:
     def __init__(self, index, slots: int = 3, max_queries_per_launch: int = 1 << 20,
                  pairs_per_launch: int = 32 << 20, max_parts_per_launch: int = 1024,
-                 hbm_budget_bytes: int = 0, host_result_bytes: int = 1 << 30):
+                 hbm_budget_bytes: int = 0, host_result_bytes: int = 1 << 30,
+                 use_graphs: bool = True):
         c = L.rts_server_config()
         check(lib().rts_server_config_default(ctypes.byref(c)))
         c.slots = slots
@@ -23,6 +24,7 @@ class Server:
         c.max_parts_per_launch = max_parts_per_launch
         c.hbm_budget_bytes = hbm_budget_bytes
         c.host_result_bytes = host_result_bytes
+        c.use_graphs = 1 if use_graphs else 0
         self.index = index
         self._h = ctypes.c_void_p()
         check(lib().rts_server_create(index._handle(), ctypes.byref(c), ctypes.byref(self._h)))

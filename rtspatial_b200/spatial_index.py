@@ -85,6 +85,7 @@ class Config:
     query_occupancy: int = 0
     frontier_factor: float = 0.0
     coord_bits: int = 32    # 64: SpatialIndex<double, 2> (float64 tensors throughout)
+    group_loads: int = L.RTS_LOADS_AUTO  # L1 use of the thread scheme's group loads
 
     def to_c(self) -> L.rts_config:
         c = L.rts_config()
@@ -305,7 +306,8 @@ class SpatialIndex:
         check(lib().rts_autotune(self._handle(), arr, len(batches), 1 if tune_width else 0,
                                  _stream_handle(stream), ctypes.byref(r)))
         res = {f: getattr(r, f) for f, _ in L.rts_tune_result._fields_}
-        for k in ("node_width", "traversal", "query_occupancy", "sort_queries", "chunk"):
+        for k in ("node_width", "traversal", "query_occupancy", "sort_queries", "chunk",
+                  "group_loads"):
             setattr(self.config, k, res[k])
         return res
 

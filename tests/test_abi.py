@@ -98,6 +98,16 @@ def test_argument_validation_without_gpu():
     c.traversal = 9
     assert lib.rts_create(ctypes.byref(c), ctypes.byref(h)) == L.RTS_ERR_INVALID_ARGUMENT
     c.traversal = L.RTS_TRAVERSAL_AUTO
+    # the L1 policy of the group loads: auto, cached, streaming
+    for gl in (L.RTS_LOADS_AUTO, L.RTS_LOADS_CACHED, L.RTS_LOADS_STREAMING):
+        c.group_loads = gl
+        h2 = ctypes.c_void_p()
+        assert lib.rts_create(ctypes.byref(c), ctypes.byref(h2)) == L.RTS_OK, gl
+        lib.rts_destroy(h2)
+    c.group_loads = 3
+    assert lib.rts_create(ctypes.byref(c), ctypes.byref(h)) == L.RTS_ERR_INVALID_ARGUMENT
+    assert b"group_loads" in lib.rts_last_error()
+    c.group_loads = L.RTS_LOADS_AUTO
     assert lib.rts_create(ctypes.byref(c), ctypes.byref(h)) == L.RTS_OK
     try:
         assert lib.rts_size(h) == 0 and lib.rts_num_trees(h) == 0

@@ -132,3 +132,26 @@ def test_server_zero_copy_views_and_stage_times(cuda, oracle):
     sv.close()
     assert st["parts"] >= st["launches"] > 0
     assert st["launch_s"] > 0 and st["copy_s"] > 0 and st["pack_s"] > 0
+
+
+def test_server_graph_replay_equals_direct_launches(cuda, oracle):
+    """Launches replayed through each slot's CUDA graph (updated in place per
+    launch) give the pairs of direct launches, for small and sorted launches."""
+    rng = np.random.default_rng(35)
+    boxes = wl.uniform_boxes(rng, 60_000, 1e-2)
+    ix = rb.SpatialIndex(rb.Config())
+    ix.Insert(dev(boxes))
+    torch.cuda.synchronize()
+    reqs = make_requests(rng, 24, max_n=30000)
+    got = {}
+    for graphs in (True, False):
+        sv = rb.Server(ix, slots=2, max_queries_per_launch=64 * 1024, pairs_per_launch=4 << 20,
+                       use_graphs=graphs)
+        tickets = [sv.submit(KIND[k][1], q) for k, q in reqs]
+        got[graphs] = [canon(sv.take(t)) for t in tickets]
+        st = sv.stats()
+        sv.close()
+        assert (st["graph_launches"] == st["launches"]) if graphs else st["graph_launches"] == 0
+    for (k, q), a, b in zip(reqs, got[True], got[False]):
+        assert np.array_equal(a, b)
+        assert_same_pairs(a, oracle.run(KIND[k][0], boxes, q)[2], "graph replay vs oracle")
