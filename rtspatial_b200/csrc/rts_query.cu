@@ -1,5 +1,6 @@
 // Query launcher: picks the kernel of a launch plan (compiled per occupancy
 // in rts_query_occ<MINB>.cu), sizes its persistent grid and launches it.
+#include <algorithm>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -61,10 +62,13 @@ static size_t dyn_smem_bytes(const LaunchPlan& p, bool merged) {
   return per * (kQueryThreads / 32);
 }
 
-// Raises the kernel's dynamic shared-memory limit (to its largest use) once
-// per device.
+// Once per kernel and device: raises the kernel's dynamic shared-memory limit
+// (to its largest use) and asks for a shared-memory carve-out no larger than
+// its resident CTAs use.  L1 and shared memory share one array per SM; the
+// query kernels are register-limited to fewer CTAs than their shared memory
+// would allow, and the unused carve-out serves better as L1 (the kernels
+// spill through it and re-read the upper tree levels from it).
 static int prepare_kernel(QueryKernel k, size_t dyn) {
-  if (dyn == 0) return RTS_OK;
   static std::mutex mu;
   static std::set<std::pair<int, const void*>> done;
   int dev = 0;
@@ -72,8 +76,20 @@ static int prepare_kernel(QueryKernel k, size_t dyn) {
   std::lock_guard<std::mutex> lock(mu);
   const auto key = std::make_pair(dev, reinterpret_cast<const void*>(k));
   if (done.count(key)) return RTS_OK;
-  RTS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(dyn)));
+  if (dyn)
+    RTS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(dyn)));
+  int blocks = 0, smem_sm = 0, reserved = 0;
+  cudaFuncAttributes fa{};
+  RTS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, kQueryThreads, dyn));
+  RTS_CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+  RTS_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  RTS_CUDA_TRY(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  if (blocks > 0 && smem_sm > 0) {
+    const size_t need = static_cast<size_t>(blocks) * (fa.sharedSizeBytes + dyn + reserved);
+    const int pct = static_cast<int>(std::min<size_t>(100, (need * 100 + smem_sm - 1) / smem_sm + 1));
+    RTS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+  }
   done.insert(key);
   return RTS_OK;
 }
