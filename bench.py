@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--traversal", type=int, default=-1)
     ap.add_argument("--curve", type=int, default=-1)
     ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--max-trees", type=int, default=0, help="sub-trees before a merge (0: library default)")
     ap.add_argument("--sort", type=int, default=-1, help="sort_queries: 0 never, 1 always, 2 auto")
     ap.add_argument("--occupancy", type=int, default=-1)
     ap.add_argument("--group-loads", type=int, default=-1,
@@ -367,7 +368,8 @@ class Ctx:
 
 def make_index(args, rb):
     cfg = rb.Config()
-    for k, v in (("node_width", args.node_width), ("chunk", args.chunk)):
+    for k, v in (("node_width", args.node_width), ("chunk", args.chunk),
+                 ("max_trees", args.max_trees)):
         if v:
             setattr(cfg, k, v)
     for k, v in (("traversal", args.traversal), ("curve", args.curve), ("sort_queries", args.sort),
