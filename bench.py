@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch settings")
     ap.add_argument("--rounds", type=int, default=0,
                     help="config 4: mutation rounds (default 50, the configuration's)")
+    ap.add_argument("--rounds-out", default="",
+                    help="config 4: write each timed round's times and sub-tree count to this "
+                         "JSON file")
     ap.add_argument("--requests", type=int, default=600, help="config 5: requests per run")
     ap.add_argument("--no-graphs", action="store_true",
                     help="config 5: the server issues its launches directly (no graph replay)")
@@ -799,6 +802,9 @@ def run_mutable_bench(args, ctx):
                 raise SystemExit(f"round {r}: mutated index differs from the oracle: {res}")
             del qu, pairs_h
     clocks_info = clocks.stop()
+    if args.rounds_out and ctx.rank == 0:
+        with open(args.rounds_out, "w") as f:
+            json.dump(rows, f, indent=0)
     step_ms = ctx.max(total_ms / rounds)
     e2e_step_ms = ctx.max(e2e_ms / rounds)
     if ctx.rank != 0:

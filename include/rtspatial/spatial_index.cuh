@@ -65,7 +65,7 @@ struct Config {
   int node_width = 16;
   int traversal = RTS_TRAVERSAL_AUTO;
   int curve = RTS_CURVE_HILBERT;
-  int max_trees = 8;
+  int max_trees = 4;
   float rebuild_fraction = 0.25f;
   float rebuild_update_fraction = 0.25f;
   uint32_t chunk = 0;

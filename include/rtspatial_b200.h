@@ -120,9 +120,10 @@ typedef struct rts_config {
   int32_t node_width;     /* children per node and boxes per leaf: 4, 8, 16 or 32 (default 16) */
   int32_t traversal;      /* RTS_TRAVERSAL_* */
   int32_t curve;          /* RTS_CURVE_*: the order leaves are packed in */
-  int32_t max_trees;      /* sub-trees kept before a merge (1..16): the sub-trees beside the
-                             largest merge into one when they hold at most an eighth of its
-                             slots, else every box is re-sorted into one tree */
+  int32_t max_trees;      /* sub-trees kept before a merge (1..16, default 4): the sub-trees
+                             beside the largest merge into one when they hold at most an
+                             eighth of its slots and fit in the slot arrays, else every box
+                             is re-sorted into one tree */
   float rebuild_fraction; /* an insert batch larger than this fraction of the index rebuilds everything */
   int32_t sort_queries;   /* visit queries in curve order (results keep the caller's query ids):
                              0 never, 1 always, 2 when a launch has >= 8192 queries */
@@ -425,6 +426,16 @@ uint64_t rts_memory_usage(const rts_index* index);
  * 0 after every launch that completed normally.  The bits stay set. */
 #define RTS_STATUS_WAIT_TIMEOUT 1u
 int rts_device_status(rts_index* index, uint32_t* status, void* stream);
+/* No counterpart in the reference.  The library's device memory on `device`
+ * (an ordinal): every device buffer of every index, plan and server comes
+ * from the library's caching allocator, which keeps freed blocks for reuse
+ * (stream-ordered: a block freed on one stream and reused on another is
+ * waited for).  `reserved` = bytes held from cudaMalloc, `used` = bytes in
+ * live buffers; both 0 before the library's first allocation there. */
+int rts_memory_pool_stats(int device, uint64_t* reserved, uint64_t* used);
+/* Returns the kept, unused blocks on `device` to the driver, after a
+ * synchronisation of that device (rts_destroy does this too). */
+int rts_trim_memory(int device);
 /* Message of the last failing call on this thread ("" if none). */
 const char* rts_last_error(void);
 /* Library version string. */

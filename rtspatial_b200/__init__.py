@@ -16,9 +16,11 @@ from .spatial_index import (  # noqa: F401
     Predicate,
     Queue,
     SpatialIndex,
+    memory_pool_stats,
     sort_pairs,
+    trim_memory,
 )
 from .server import Server  # noqa: F401
 
 __all__ = ["Config", "Counter", "Handler", "Plan", "Predicate", "Queue", "SpatialIndex", "sort_pairs",
-           "RtsError", "lib", "LIB_PATH", "Server"]
+           "memory_pool_stats", "trim_memory", "RtsError", "lib", "LIB_PATH", "Server"]

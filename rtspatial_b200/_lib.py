@@ -171,6 +171,8 @@ SIGNATURES = {
     "rts_size": (_U64, [_P]),
     "rts_num_trees": (ctypes.c_uint32, [_P]),
     "rts_memory_usage": (_U64, [_P]),
+    "rts_memory_pool_stats": (_I, [_I, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "rts_trim_memory": (_I, [_I]),
     "rts_last_error": (ctypes.c_char_p, []),
     "rts_version": (ctypes.c_char_p, []),
 }

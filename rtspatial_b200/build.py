@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "librtspatial_b200.so")
 SOURCES = ["rts_query_occ1.cu", "rts_query_occ2.cu", "rts_query_occ3.cu", "rts_query_occ4.cu",
            "rts_query_staged.cu",
            "rts_index.cu", "rts_plan.cu", "rts_server.cu", "rts_tune.cu", "rts_frontier.cu",
-           "rts_query.cu", "rts_build.cu"]
+           "rts_query.cu", "rts_build.cu", "rts_memory.cu"]
 HEADERS = ["rts_device.cuh", "rts_traverse.cuh", "rts_query_kernels.cuh", "rts_internal.h",
            "rts_index_impl.h", "rts_handler_kernel.cuh"]
 

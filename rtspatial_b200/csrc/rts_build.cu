@@ -427,6 +427,17 @@ int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_
   return RTS_OK;
 }
 
+int reserve_sort_temp(uint64_t n, DevBuf& temp, cudaStream_t s) {
+  if (n == 0) return RTS_OK;
+  size_t need = 0;
+  RTS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, static_cast<const uint32_t*>(nullptr),
+                                                static_cast<uint32_t*>(nullptr),
+                                                static_cast<const uint32_t*>(nullptr),
+                                                static_cast<uint32_t*>(nullptr),
+                                                static_cast<int>(n), 0, 32, s));
+  return buf_reserve(temp, need, s, false, 0);
+}
+
 int launch_gather(const float4* src, const uint32_t* src_ids, const uint32_t* order, uint64_t n,
                   uint64_t id_begin, uint64_t slot_base, float4* leaves, uint32_t* leaf_ids,
                   uint32_t* pos, cudaStream_t s, const DBox* src64, DBox* leaves64,

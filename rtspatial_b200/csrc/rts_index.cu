@@ -38,43 +38,6 @@ int cuda_fail(cudaError_t e, const char* what) {
   return (e == cudaErrorMemoryAllocation) ? RTS_ERR_OUT_OF_MEMORY : RTS_ERR_CUDA;
 }
 
-// The stream-ordered allocator returns freed blocks to the system at every
-// synchronisation unless told otherwise; re-sorts free and reallocate
-// hundreds of MB, so keep freed blocks in the device's default pool.
-void keep_pool_memory() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
-  uint64_t keep = ~0ull;
-  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-}
-
-int buf_reserve(DevBuf& b, size_t bytes, cudaStream_t s, bool keep, size_t used) {
-  if (bytes <= b.bytes && b.ptr) return RTS_OK;
-  size_t cap = std::max(bytes, b.bytes + b.bytes / 2);
-  cap = (cap + 255) & ~static_cast<size_t>(255);
-  void* p = nullptr;
-  RTS_CUDA_TRY(cudaMallocAsync(&p, cap, s));
-  if (keep && b.ptr && used) {
-    cudaError_t e = cudaMemcpyAsync(p, b.ptr, std::min(used, b.bytes), cudaMemcpyDeviceToDevice, s);
-    if (e != cudaSuccess) {
-      cudaFreeAsync(p, s);
-      return cuda_fail(e, "cudaMemcpyAsync(grow)");
-    }
-  }
-  if (b.ptr) cudaFreeAsync(b.ptr, s);
-  b.ptr = p;
-  b.bytes = cap;
-  return RTS_OK;
-}
-
-void buf_free(DevBuf& b, cudaStream_t s) {
-  if (b.ptr) cudaFreeAsync(b.ptr, s);
-  b.ptr = nullptr;
-  b.bytes = 0;
-}
-
 // Levels storable by the traversal's mask stack at each width.
 static uint32_t max_levels_for(int W) {
   switch (W) {
@@ -92,26 +55,18 @@ using namespace rts;
 
 namespace rts {
 
-int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
-  uint64_t need = slots + kSlotAlign;
-  int rc;
-  if (!ix->status.ptr) {  // the device status word the query kernels report into
-    if ((rc = buf_reserve(ix->status, sizeof(uint32_t), s, false, 0))) return rc;
-    RTS_CUDA_TRY(cudaMemsetAsync(ix->status.ptr, 0, sizeof(uint32_t), s));
-    ix->forest_dirty = true;
-  }
-  rc = buf_reserve(ix->leaves, need * sizeof(float4), s, true, ix->slot_end * sizeof(float4));
-  if (rc) return rc;
-  if (is_f64(ix) &&
-      (rc = buf_reserve(ix->leaves64, need * sizeof(DBox), s, true, ix->slot_end * sizeof(DBox))))
-    return rc;
-  return buf_reserve(ix->leaf_ids, need * sizeof(uint32_t), s, true,
-                     ix->slot_end * sizeof(uint32_t));
-}
-
-int ensure_ids(rts_index* ix, uint64_t ids, cudaStream_t s) {
-  return buf_reserve(ix->pos, std::max<uint64_t>(ids, 1) * sizeof(uint32_t), s, true,
-                     ix->n_ids * sizeof(uint32_t));
+// Capacity a growing slot or id array asks for: exactly `need` the first
+// time (an index built once stays tight), then at least twice the current
+// capacity below 4 GB and a quarter more above.  With the re-sort buffers
+// reserved alongside (reserve_for_resort), an index under rounds of updates
+// and inserts allocates only when its ids or slots pass a capacity, not on
+// every merge or re-sort: device allocations were measured on B200 to stall
+// the host for tens to hundreds of ms at random (the driver maps memory under
+// a lock the GPU's other processes share).
+static size_t grown_bytes(const DevBuf& b, size_t need) {
+  if (need <= b.bytes || b.bytes == 0) return need;
+  const size_t cap = b.bytes < (4ull << 30) ? 2 * b.bytes : b.bytes + b.bytes / 4;
+  return std::max(need, cap);
 }
 
 int ensure_sort_scratch(rts_index* ix, uint64_t n, cudaStream_t s) {
@@ -122,6 +77,58 @@ int ensure_sort_scratch(rts_index* ix, uint64_t n, cudaStream_t s) {
   if ((rc = buf_reserve(ix->vals_a, b, s, false, 0))) return rc;
   if ((rc = buf_reserve(ix->vals_b, b, s, false, 0))) return rc;
   return buf_reserve(ix->bounds, 4 * sizeof(uint32_t), s, false, 0);
+}
+
+// Everything a full re-sort, a merge or an update split of an index within
+// its current capacities uses: spare slot arrays as large as the slot arrays,
+// and sort keys, values, sort temp and the slot list for as many ids as the
+// id map holds.  Called when a slot or id array of a non-empty index grows.
+static int reserve_for_resort(rts_index* ix, cudaStream_t s) {
+  int rc;
+  if ((rc = buf_reserve(ix->spare_leaves, ix->leaves.bytes, s, false, 0)) ||
+      (rc = buf_reserve(ix->spare_ids, ix->leaf_ids.bytes, s, false, 0)) ||
+      (is_f64(ix) && (rc = buf_reserve(ix->spare_leaves64, ix->leaves64.bytes, s, false, 0))))
+    return rc;
+  const uint64_t ids = ix->pos.bytes / sizeof(uint32_t);
+  const uint64_t slots = ix->leaf_ids.bytes / sizeof(uint32_t);
+  HostTree full;
+  plan_levels(ids, ix->W, full);
+  if ((rc = buf_reserve(ix->spare_nodes, full.node_entries * sizeof(float4), s, false, 0)))
+    return rc;
+  if ((rc = ensure_sort_scratch(ix, ids, s)) || (rc = reserve_sort_temp(ids, ix->sort_temp, s)) ||
+      (rc = buf_reserve(ix->slots_tmp, std::max<uint64_t>(ids, 1) * sizeof(uint32_t), s, false, 0)) ||
+      (rc = buf_reserve(ix->upd_bits, 2 * ((slots + 31) / 32) * sizeof(uint32_t), s, false, 0)))
+    return rc;
+  return RTS_OK;
+}
+
+int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
+  uint64_t need = slots + kSlotAlign;
+  int rc;
+  if (!ix->status.ptr) {  // the device status word the query kernels report into
+    if ((rc = buf_reserve(ix->status, sizeof(uint32_t), s, false, 0))) return rc;
+    RTS_CUDA_TRY(cudaMemsetAsync(ix->status.ptr, 0, sizeof(uint32_t), s));
+    ix->forest_dirty = true;
+  }
+  const bool grow = need * sizeof(uint32_t) > ix->leaf_ids.bytes;
+  const uint64_t cap = grown_bytes(ix->leaf_ids, need * sizeof(uint32_t)) / sizeof(uint32_t);
+  rc = buf_reserve(ix->leaves, cap * sizeof(float4), s, true, ix->slot_end * sizeof(float4));
+  if (rc) return rc;
+  if (is_f64(ix) &&
+      (rc = buf_reserve(ix->leaves64, cap * sizeof(DBox), s, true, ix->slot_end * sizeof(DBox))))
+    return rc;
+  if ((rc = buf_reserve(ix->leaf_ids, cap * sizeof(uint32_t), s, true,
+                        ix->slot_end * sizeof(uint32_t))))
+    return rc;
+  return grow && !ix->trees.empty() ? reserve_for_resort(ix, s) : RTS_OK;
+}
+
+int ensure_ids(rts_index* ix, uint64_t ids, cudaStream_t s) {
+  const size_t need = std::max<uint64_t>(ids, 1) * sizeof(uint32_t);
+  const bool grow = need > ix->pos.bytes;
+  int rc = buf_reserve(ix->pos, grown_bytes(ix->pos, need), s, true, ix->n_ids * sizeof(uint32_t));
+  if (rc) return rc;
+  return grow && !ix->trees.empty() ? reserve_for_resort(ix, s) : RTS_OK;
 }
 
 float4* leaves_of(rts_index* ix) { return static_cast<float4*>(ix->leaves.ptr); }
@@ -192,43 +199,39 @@ int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
   if ((rc = buf_reserve(ix->slots_tmp, N * sizeof(uint32_t), s, false, 0))) return rc;
   auto* slots = static_cast<uint32_t*>(ix->slots_tmp.ptr);
   RTS_CUDA_TRY(cudaMemcpyAsync(slots, pos_of(ix), N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-  // New slot arrays; the old ones are read by the gather.
-  DevBuf new_leaves, new_ids, new_leaves64;
+  // The boxes are gathered into the spare slot arrays, which then become the
+  // index's (the old ones are read by the gather and kept as the next spare).
   const uint64_t slots_needed = round_up(N, kSlotAlign);
-  auto drop = [&]() {
-    buf_free(new_leaves, s);
-    buf_free(new_ids, s);
-    buf_free(new_leaves64, s);
-  };
-  if ((rc = buf_reserve(new_leaves, std::max(ix->leaves.bytes, (slots_needed + kSlotAlign) * sizeof(float4)), s, false, 0)))
+  const uint64_t cap = std::max<uint64_t>(ix->leaf_ids.bytes / sizeof(uint32_t), slots_needed + kSlotAlign);
+  if ((rc = buf_reserve(ix->spare_leaves, cap * sizeof(float4), s, false, 0)) ||
+      (rc = buf_reserve(ix->spare_ids, cap * sizeof(uint32_t), s, false, 0)) ||
+      (is_f64(ix) && (rc = buf_reserve(ix->spare_leaves64, cap * sizeof(DBox), s, false, 0))))
     return rc;
-  if ((rc = buf_reserve(new_ids, std::max(ix->leaf_ids.bytes, (slots_needed + kSlotAlign) * sizeof(uint32_t)), s, false, 0))) {
-    drop();
-    return rc;
-  }
-  if (is_f64(ix) &&
-      (rc = buf_reserve(new_leaves64, std::max(ix->leaves64.bytes, (slots_needed + kSlotAlign) * sizeof(DBox)), s, false, 0))) {
-    drop();
-    return rc;
-  }
   rc = sort_into_slots(ix, leaves_of(ix), ids_of(ix), slots, N, 0, 0,
-                       static_cast<float4*>(new_leaves.ptr), static_cast<uint32_t*>(new_ids.ptr), s,
-                       leaves64_of(ix), is_f64(ix) ? static_cast<DBox*>(new_leaves64.ptr) : nullptr);
-  if (rc) {
-    drop();
-    return rc;
-  }
-  buf_free(ix->leaves, s);
-  buf_free(ix->leaf_ids, s);
-  ix->leaves = new_leaves;
-  ix->leaf_ids = new_ids;
-  if (is_f64(ix)) {
-    buf_free(ix->leaves64, s);
-    ix->leaves64 = new_leaves64;
-  }
-  for (auto& t : ix->trees) buf_free(t.nodes, s);
-  ix->trees.clear();
+                       static_cast<float4*>(ix->spare_leaves.ptr),
+                       static_cast<uint32_t*>(ix->spare_ids.ptr), s, leaves64_of(ix),
+                       is_f64(ix) ? static_cast<DBox*>(ix->spare_leaves64.ptr) : nullptr);
+  if (rc) return rc;
+  std::swap(ix->leaves, ix->spare_leaves);
+  std::swap(ix->leaf_ids, ix->spare_ids);
+  if (is_f64(ix)) std::swap(ix->leaves64, ix->spare_leaves64);
+  // The new tree is built in the spare node buffer; the largest old one
+  // becomes the spare, the others are freed.
   HostTree t;
+  t.nodes = ix->spare_nodes;
+  ix->spare_nodes = DevBuf{};
+  size_t big = 0;
+  for (size_t i = 1; i < ix->trees.size(); ++i)
+    if (ix->trees[i].nodes.bytes > ix->trees[big].nodes.bytes) big = i;
+  for (size_t i = 0; i < ix->trees.size(); ++i) {
+    if (i == big) {
+      ix->spare_nodes = ix->trees[i].nodes;
+      ix->trees[i].nodes = DevBuf{};
+    } else {
+      buf_free(ix->trees[i].nodes, s);
+    }
+  }
+  ix->trees.clear();
   t.id_begin = 0;
   t.n = N;
   t.slot_base = 0;
@@ -248,7 +251,10 @@ int rebuild_all_impl(rts_index* ix, cudaStream_t s) {
 // emptied by moved updates come along as NaN boxes, which answer nothing, and
 // pos[] moves only for ids whose envelope a slot still holds.  The old slots
 // stay unused until the next full re-sort.  Beyond an eighth, queries would
-// walk a second large tree, and a full re-sort is due instead.
+// walk a second large tree, and a full re-sort is due instead; so is it when
+// the merged slots would not fit in the slot arrays (the re-sort compacts the
+// slots, where a merge would grow the arrays: an allocation on the update
+// path).
 static bool small_trees_mergeable(const rts_index* ix) {
   const auto& tr = ix->trees;
   if (tr.size() < 3 || ix->cfg.max_trees < 2) return false;
@@ -260,7 +266,9 @@ static bool small_trees_mergeable(const rts_index* ix) {
   for (size_t i = 0; i < tr.size(); ++i)
     if (i != big) m += tr[i].n;
   const uint64_t end = ix->slot_end + round_up(m, kSlotAlign);
-  return 8 * m <= tr[big].n && end <= 2 * ix->n_ids + (1u << 20) && end < 0xffffffffull - kSlotAlign;
+  const uint64_t room = ix->leaf_ids.bytes / sizeof(uint32_t);
+  return 8 * m <= tr[big].n && end <= 2 * ix->n_ids + (1u << 20) && end + kSlotAlign <= room &&
+         end < 0xffffffffull - kSlotAlign;
 }
 
 static int merge_small_trees(rts_index* ix, cudaStream_t s) {
@@ -690,7 +698,7 @@ int rts_config_default(rts_config* c) {
   c->node_width = 16;
   c->traversal = RTS_TRAVERSAL_AUTO;
   c->curve = RTS_CURVE_HILBERT;
-  c->max_trees = 8;
+  c->max_trees = 4;
   c->rebuild_fraction = 0.25f;
   c->sort_queries = 2;
   c->query_occupancy = 0;
@@ -720,7 +728,6 @@ int rts_create(const rts_config* cfg, rts_index** out) {
     return fail(RTS_ERR_INVALID_ARGUMENT, "coord_bits must be 32 or 64");
   auto* ix = new (std::nothrow) rts_index();
   if (!ix) return fail(RTS_ERR_OUT_OF_MEMORY, "host allocation failed");
-  keep_pool_memory();
   ix->cfg = c;
   ix->W = c.node_width;
   if (c.preallocate && c.max_geometries) {
@@ -745,6 +752,7 @@ int rts_destroy(rts_index* ix) {
   }
   DevBuf* all[] = {&ix->leaves, &ix->leaf_ids, &ix->pos, &ix->keys_a, &ix->keys_b, &ix->vals_a,
                    &ix->vals_b, &ix->sort_temp, &ix->bounds, &ix->slots_tmp, &ix->leaves64,
+                   &ix->spare_leaves, &ix->spare_ids, &ix->spare_leaves64, &ix->spare_nodes,
                    &ix->rounded, &ix->upd_bits, &ix->upd_ids, &ix->upd_boxes,
                    &ix->upd_boxes64, &ix->upd_count, &ix->status};
   for (DevBuf* b : all) {
@@ -760,7 +768,11 @@ int rts_destroy(rts_index* ix) {
   touched |= ix->qs.work.ptr != nullptr;
   ix->qs.release(s);
   ix->staging.release();
-  if (touched) cudaStreamSynchronize(s);  // frees are stream-ordered
+  if (touched) {
+    cudaStreamSynchronize(s);  // frees are stream-ordered
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) rts_trim_memory(dev);
+  }
   delete ix;
   return RTS_OK;
 }
@@ -1104,7 +1116,9 @@ uint32_t rts_num_trees(const rts_index* ix) {
 
 uint64_t rts_memory_usage(const rts_index* ix) {
   if (!ix) return 0;
-  uint64_t b = ix->leaves.bytes + ix->leaf_ids.bytes + ix->pos.bytes + ix->leaves64.bytes;
+  uint64_t b = ix->leaves.bytes + ix->leaf_ids.bytes + ix->pos.bytes + ix->leaves64.bytes +
+               ix->spare_leaves.bytes + ix->spare_ids.bytes + ix->spare_leaves64.bytes +
+               ix->spare_nodes.bytes;
   for (const auto& t : ix->trees) b += t.nodes.bytes;
   return b;
 }

@@ -98,6 +98,12 @@ struct rts_index {
   cudaKernel_t hkern[4] = {};
   int hmod_builtin = -1;
   rts::DevBuf leaves64;         // double index: the double envelopes, slot by slot
+  // a full re-sort gathers into these and swaps them with leaves / leaf_ids /
+  // leaves64 (reserved with them once the index is mutated; see ensure_slots)
+  rts::DevBuf spare_leaves, spare_ids, spare_leaves64;
+  // node buffer the next full re-sort builds its tree in (the previous
+  // largest sub-tree's buffer, or reserved for the id capacity)
+  rts::DevBuf spare_nodes;
   rts::DevBuf rounded;          // double index: scratch of an insert's float rounding
   // scratch of the update split: slot bitmaps, moved ids / envelopes, count
   rts::DevBuf upd_bits, upd_ids, upd_boxes, upd_boxes64, upd_count;
@@ -137,7 +143,6 @@ uint64_t sum_queries(const rts_batch* batches, uint32_t n);
 // kIntersects when every batch is a range-intersects batch, else kContains
 // (the predicate plan_for picks the default traversal scheme by).
 int launch_pred(const rts_batch* batches, uint32_t n);
-void keep_pool_memory();
 bool want_sort(const rts_index* ix, uint64_t total);
 int check_handler(int handler, void* arg);
 // The kernel-side handler (kCount, kCollect or kUser) of a public handler kind.

@@ -28,6 +28,11 @@ struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
 };
+// Device memory (rts_memory.cu): the library's caching allocator on the
+// current device.  A block is usable on stream s in stream order; dev_free
+// hands it back once the work queued on s before the free is done.
+int dev_alloc(void** p, size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
 int buf_reserve(DevBuf& b, size_t bytes, cudaStream_t s, bool keep_contents, size_t used_bytes);
 void buf_free(DevBuf& b, cudaStream_t s);
 
@@ -56,6 +61,8 @@ int launch_curve_keys(const float4* boxes, const uint32_t* idx, uint64_t n, cons
                       int curve, uint32_t* keys, uint32_t* vals, cudaStream_t s);
 int sort_pairs(const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
                uint64_t n, DevBuf& temp, cudaStream_t s);
+// Reserves `temp` for a sort_pairs of up to n pairs.
+int reserve_sort_temp(uint64_t n, DevBuf& temp, cudaStream_t s);
 // For i < n with o = order[i]: leaves[slot_base+i] = src[o];
 // id = src_ids ? src_ids[o] : id_begin + o; leaf_ids[slot_base+i] = id;
 // pos[id] = slot_base + i (live_only: only where pos[id] == o, i.e. slot o

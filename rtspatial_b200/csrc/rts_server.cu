@@ -547,9 +547,8 @@ void release_chunks(rts_server* sv, Request* r) {
 // submitted before the update has its final pairs and every later query
 // launches after it (its stream waits on ev_update).
 int stage_and(cudaStream_t us, const void* host, size_t bytes, void** dev) {
-  *dev = nullptr;
-  cudaError_t e = cudaMallocAsync(dev, bytes, us);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, us);
+  if (int rc = dev_alloc(dev, bytes, us)) return rc;
+  cudaError_t e = cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, us);
   if (e != cudaSuccess) return cuda_fail(e, "staging an update batch");
   return RTS_OK;
 }
@@ -562,19 +561,19 @@ void apply_update(rts_server* sv, Request* r) {
   if (!r->del.empty()) {
     rc = stage_and(us, r->del.data(), r->del.size() * sizeof(uint64_t), &d);
     if (!rc) rc = rts_delete(sv->ix, static_cast<const uint64_t*>(d), r->del.size(), us);
-    if (d) cudaFreeAsync(d, us);
+    dev_free(d, us);
   }
   if (!rc && !r->upd.empty()) {
     rc = stage_and(us, r->upd.data(), r->upd.size() * sizeof(rts_update_entry), &d);
     if (!rc) rc = rts_update(sv->ix, static_cast<const rts_update_entry*>(d), r->upd.size(), us);
-    if (d) cudaFreeAsync(d, us);
+    dev_free(d, us);
   }
   if (!rc && !r->ins.empty()) {
     const uint64_t n = r->ins.size() / 4;
     rc = stage_and(us, r->ins.data(), n * 4 * sizeof(float), &d);
     r->first_new_id = rts_size(sv->ix);
     if (!rc) rc = rts_insert(sv->ix, static_cast<const float*>(d), n, us);
-    if (d) cudaFreeAsync(d, us);
+    dev_free(d, us);
   }
   r->status = rc;
   sv->update_s += now_s() - t0;

@@ -77,7 +77,7 @@ class Config:
     node_width: int = 16
     traversal: int = L.RTS_TRAVERSAL_AUTO
     curve: int = L.RTS_CURVE_HILBERT
-    max_trees: int = 8
+    max_trees: int = 4
     rebuild_fraction: float = 0.25
     sort_queries: int = 2
     rebuild_update_fraction: float = 0.25
@@ -406,3 +406,18 @@ def sort_pairs(p: torch.Tensor) -> torch.Tensor:
         return p.reshape(0, 2)
     key = p[:, 1] * (1 << 32) + p[:, 0]
     return p[torch.argsort(key)]
+
+
+def memory_pool_stats(device: int | None = None) -> tuple:
+    """(reserved, used) bytes of the library's device-memory pool on `device`
+    (default: the current CUDA device)."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    r, u = ctypes.c_uint64(), ctypes.c_uint64()
+    check(lib().rts_memory_pool_stats(dev, ctypes.byref(r), ctypes.byref(u)))
+    return int(r.value), int(u.value)
+
+
+def trim_memory(device: int | None = None) -> None:
+    """Returns the unused part of the library's pool on `device` to the driver."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    check(lib().rts_trim_memory(dev))

@@ -7,9 +7,9 @@ manager.  For them the library offers a batched query whose scratch (work
 counter and descriptor copy) is a fixed array inside the library.  These
 tests call it through the C-ABI and check that two calls in a row give
 exactly the pairs and counts of the regular rts_query_batched, on a float and
-on a double index; that neither call moves the device's stream-ordered pool
-(where the library's own allocations come from) nor, once the first call has
-looked up the fixed array, the device's free memory; that it rejects what
+on a double index; that neither call moves the library's caching allocator
+(where its own allocations come from) or the device's default pool nor,
+once the first call has looked up the fixed array, the device's free memory; that it rejects what
 rts_query_batched rejects; and that it refuses more non-empty batches than
 its fixed scratch holds.  Each test builds its own index, so the file runs the
 same alone in a fresh process or after the other tests.
@@ -44,7 +44,9 @@ def _batches(specs, queues):
 
 
 def _pool_bytes() -> tuple:
-    """(used, reserved) bytes of the current device's default memory pool."""
+    """(used, reserved) bytes of the current device's default memory pool and
+    of the library's caching allocator (where every library allocation comes
+    from)."""
     err, dev = cudart.cudaGetDevice()
     assert err == cudart.cudaError_t.cudaSuccess
     err, pool = cudart.cudaDeviceGetDefaultMemPool(dev)
@@ -55,7 +57,9 @@ def _pool_bytes() -> tuple:
         err, v = cudart.cudaMemPoolGetAttribute(pool, attr)
         assert err == cudart.cudaError_t.cudaSuccess
         out.append(int(v))
-    return tuple(out)
+    reserved, used = rb.memory_pool_stats(dev)
+    assert reserved >= used > 0  # the index's buffers live there
+    return tuple(out) + (used, reserved)
 
 
 def _free_bytes() -> int:
@@ -92,7 +96,7 @@ def _check_against_regular(ix, specs):
         for i, (g, w) in enumerate(zip(got_qs[call], want)):
             assert g.size() <= g.capacity()
             assert np.array_equal(_canon(g), w), f"call {call}, batch {i}"
-    assert pool2 == pool0, "the no-allocation call took memory from the device pool"
+    assert pool2 == pool0, "the no-allocation call took memory from a device pool"
     assert free2 == free1, "the second no-allocation call changed the free device memory"
 
 
