@@ -1186,7 +1186,7 @@ def run_config(args, ctx):
 
 # Reduced runs of the other configurations that the default (config 2) run
 # nests in its line: full-size inputs, fewer steps.
-OTHER_CONFIGS = {1: dict(steps=10), 3: dict(steps=10), 4: dict(rounds=4, warmup=1),
+OTHER_CONFIGS = {1: dict(steps=10), 3: dict(steps=10), 4: dict(rounds=5, warmup=3),
                  5: dict(requests=200)}
 
 

@@ -320,9 +320,17 @@ __device__ __forceinline__ bool isect_leaf(float4 g, const IsectQuery& Q) {
 // computed once, and its diagonal reciprocals the first time a query passes
 // the prefilter (gix, giy, have carry them between calls).  The same
 // operations as isect_leaf, so the same results.
+__device__ __forceinline__ bool isect_leaf_post(float4 g, float& gix, float& giy, bool& have,
+                                                const IsectQuery& Q);
 __device__ __forceinline__ bool isect_leaf_pre(float4 g, float4 h, float& gix, float& giy,
                                                bool& have, const IsectQuery& Q) {
   if (!overlaps(h, Q.nb)) return false;
+  return isect_leaf_post(g, gix, giy, have, Q);
+}
+
+// The part of isect_leaf_pre after its hull prefilter passed.
+__device__ __forceinline__ bool isect_leaf_post(float4 g, float& gix, float& giy, bool& have,
+                                                const IsectQuery& Q) {
   if (!have) {
     gix = __frcp_rn(__fsub_rn(g.z, g.x));
     giy = __frcp_rn(__fsub_rn(g.w, g.y));

@@ -491,6 +491,13 @@ namespace rts {
 // per query, and every lane of a round does useful work.  The tests are the
 // ones the other schemes make (node test at upper levels, exact predicate at
 // the leaves), so results are identical.
+// Position of the highest set bit of a non-zero word (one bfind).
+__device__ __forceinline__ uint32_t high_bit(uint32_t x) {
+  uint32_t r;
+  asm("bfind.u32 %0, %1;" : "=r"(r) : "r"(x));
+  return r;
+}
+
 template <int PRED, int W>
 struct PacketSmem {
   typename QueryOps<PRED>::Q q[32];  // the packet's queries (prepared per sub-tree)
@@ -599,17 +606,64 @@ __device__ __forceinline__ void run_chunk_packet(const Forest& F, const BatchDes
           }
         };
         if constexpr (kGroups == 1) {
-          while (rm) {  // uniform: two queries per round
-            const uint32_t j1 = __ffs(rm) - 1;
-            rm &= rm - 1;
-            uint32_t j2 = 32;
-            if (rm) {
-              j2 = __ffs(rm) - 1;
-              rm &= rm - 1;
+          bool done = false;
+          if constexpr (PRED == kIntersects) {
+            if (at_leaf) {
+              // Two phases: the hull prefilter of every live query gives each
+              // lane its candidates, then every lane takes its own candidates
+              // one per round through the exact (slab) test, so a round pays
+              // one exact test for up to 32 candidates of different lanes.
+              uint32_t cand = 0;
+              if (valid) {
+                if (rm == kFull) {
+#pragma unroll 4
+                  for (uint32_t j = 0; j < 32; ++j)
+                    if (overlaps(eh, P.q[j].nb)) cand |= 1u << j;
+                } else {
+                  for (uint32_t m = rm; m;) {
+                    const uint32_t j = high_bit(m);
+                    m ^= 1u << j;
+                    if (overlaps(eh, P.q[j].nb)) cand |= 1u << j;
+                  }
+                }
+              }
+              while (__any_sync(kFull, cand != 0)) {
+                if (cand) {
+                  const uint32_t j = high_bit(cand);
+                  cand ^= 1u << j;
+                  if (isect_leaf_post(e, gix, giy, have_rcp, P.q[j])) hm |= 1u << j;
+                }
+              }
+              done = true;
             }
+          }
+          // Measured on range-intersects, 10M x 1M (B200): 1.170 ms per step
+          // with one loop for all levels, 1.143 ms with the full-packet loop,
+          // 0.989 ms with the two leaf phases as well; full-packet loops also
+          // for packets with >= 20 (or 12) live queries, with a bit test per
+          // position, were slower (1.049, 1.074 ms).
+          if (done) {
+          } else if (rm == kFull) {
+            // uniform: all 32 queries in turn, no mask arithmetic (the top
+            // levels, where every query of a sorted packet is live)
             if (valid) {
-              if (test(j1)) hm |= 1u << j1;
-              if (j2 < 32 && test(j2)) hm |= 1u << j2;
+#pragma unroll 4
+              for (uint32_t j = 0; j < 32; ++j)
+                if (test(j)) hm |= 1u << j;
+            }
+          } else {
+            while (rm) {  // uniform: two queries per round, highest bits first
+              const uint32_t j1 = high_bit(rm);
+              rm ^= 1u << j1;
+              uint32_t j2 = 32;
+              if (rm) {
+                j2 = high_bit(rm);
+                rm ^= 1u << j2;
+              }
+              if (valid) {
+                if (test(j1)) hm |= 1u << j1;
+                if (j2 < 32 && test(j2)) hm |= 1u << j2;
+              }
             }
           }
         } else {
