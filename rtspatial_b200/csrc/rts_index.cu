@@ -123,6 +123,21 @@ int ensure_slots(rts_index* ix, uint64_t slots, cudaStream_t s) {
   return grow && !ix->trees.empty() ? reserve_for_resort(ix, s) : RTS_OK;
 }
 
+int ensure_ids(rts_index* ix, uint64_t ids, cudaStream_t s);
+
+// For an index about to take updates (a serving engine over it): the
+// capacity its first mutations would allocate on their way, twice the used
+// slots and ids and the re-sort buffers, reserved now.
+int reserve_for_updates(rts_index* ix, cudaStream_t s) {
+  if (ix->trees.empty()) return RTS_OK;
+  int rc;
+  const uint64_t slots_cap = ix->leaf_ids.bytes / sizeof(uint32_t);
+  const uint64_t ids_cap = ix->pos.bytes / sizeof(uint32_t);
+  if (slots_cap < 2 * ix->slot_end && (rc = ensure_slots(ix, slots_cap, s))) return rc;
+  if (ids_cap < 2 * ix->n_ids && (rc = ensure_ids(ix, ids_cap + 1, s))) return rc;
+  return reserve_for_resort(ix, s);
+}
+
 int ensure_ids(rts_index* ix, uint64_t ids, cudaStream_t s) {
   const size_t need = std::max<uint64_t>(ids, 1) * sizeof(uint32_t);
   const bool grow = need > ix->pos.bytes;
@@ -803,6 +818,16 @@ int insert_impl(rts_index* ix, const float4* src, const DBox* src64, const uint3
   if (!ids && ix->n_ids + n >= 0xffffffffull)
     return fail(RTS_ERR_CAPACITY, "ids are 32-bit: at most 2^32-2 envelopes per index");
   int rc;
+  // A sub-tree that does not fit behind the used slots, when the live boxes
+  // and it would fit once compacted: re-sort first (a few ms) instead of
+  // growing the slot arrays (an allocation of the index's size).  Merges
+  // fill the arrays up to their capacity, so an index under updates and
+  // inserts reaches this point between full re-sorts.
+  const uint64_t room = ix->leaf_ids.bytes / sizeof(uint32_t);
+  if (!ix->trees.empty() && ix->slot_end + round_up(n, kSlotAlign) + kSlotAlign > room &&
+      round_up(ix->n_ids, kSlotAlign) + round_up(n, kSlotAlign) + kSlotAlign <= room &&
+      (rc = rebuild_all(ix, s)))
+    return rc;
   const uint64_t slot_base = ix->slot_end;
   const uint64_t slot_end = slot_base + round_up(n, kSlotAlign);
   if ((rc = ensure_slots(ix, slot_end, s))) return rc;

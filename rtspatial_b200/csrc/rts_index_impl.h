@@ -144,6 +144,8 @@ uint64_t sum_queries(const rts_batch* batches, uint32_t n);
 // (the predicate plan_for picks the default traversal scheme by).
 int launch_pred(const rts_batch* batches, uint32_t n);
 bool want_sort(const rts_index* ix, uint64_t total);
+// Reserves the capacity an index's first updates would allocate (rts_index.cu).
+int reserve_for_updates(rts_index* ix, cudaStream_t s);
 int check_handler(int handler, void* arg);
 // The kernel-side handler (kCount, kCollect or kUser) of a public handler kind.
 int resolve_handler(const rts_index* ix, int handler, int* mode);

@@ -167,6 +167,13 @@ struct rts_server {
   PinnedArena arena;
   cudaStream_t update_stream = nullptr;
   cudaEvent_t ev_update = nullptr;
+  // pinned staging of update batches, two buffers used in turn; ev_staged[k]
+  // is recorded after the copies that read buffer k
+  unsigned char* upd_host[2] = {nullptr, nullptr};
+  size_t upd_host_bytes[2] = {0, 0};
+  cudaEvent_t ev_staged[2] = {nullptr, nullptr};
+  bool staged[2] = {false, false};
+  int upd_flip = 0;
   bool update_pending_event = false;  // ev_update recorded; slots must wait on it once
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -542,39 +549,82 @@ void release_chunks(rts_server* sv, Request* r) {
   r->out.clear();
 }
 
+// The parts of an update batch go through a pinned buffer of the server: a
+// copy from the request's pageable vectors would block the worker until the
+// driver had staged it, behind whatever pair copies of earlier launches are
+// still running.  Two buffers in turn, so an update only waits for the
+// copies of the one before the previous.
+int stage_update(rts_server* sv, const Request* r, void** d_del, void** d_upd, void** d_ins) {
+  cudaStream_t us = sv->update_stream;
+  const size_t b_del = r->del.size() * sizeof(uint64_t);
+  const size_t b_upd = r->upd.size() * sizeof(rts_update_entry);
+  const size_t b_ins = r->ins.size() * sizeof(float);
+  const auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t o_upd = al(b_del), o_ins = o_upd + al(b_upd), total = o_ins + b_ins;
+  const int k = sv->upd_flip;
+  sv->upd_flip ^= 1;
+  if (sv->staged[k]) RTS_CUDA_TRY(cudaEventSynchronize(sv->ev_staged[k]));
+  if (total > sv->upd_host_bytes[k]) {
+    if (sv->upd_host[k]) cudaFreeHost(sv->upd_host[k]);
+    sv->upd_host[k] = nullptr;
+    sv->upd_host_bytes[k] = 0;
+    const size_t cap = std::max(total, 2 * sv->upd_host_bytes[k ^ 1]);
+    RTS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sv->upd_host[k]), cap));
+    sv->upd_host_bytes[k] = cap;
+  }
+  unsigned char* h = sv->upd_host[k];
+  const struct {
+    const void* src;
+    size_t bytes, off;
+    void** dev;
+  } parts[3] = {{r->del.data(), b_del, 0, d_del},
+                {r->upd.data(), b_upd, o_upd, d_upd},
+                {r->ins.data(), b_ins, o_ins, d_ins}};
+  for (const auto& p : parts) {
+    *p.dev = nullptr;
+    if (!p.bytes) continue;
+    std::memcpy(h + p.off, p.src, p.bytes);
+    if (int rc = dev_alloc(p.dev, p.bytes, us)) return rc;
+    cudaError_t e = cudaMemcpyAsync(*p.dev, h + p.off, p.bytes, cudaMemcpyHostToDevice, us);
+    if (e != cudaSuccess) return cuda_fail(e, "staging an update batch");
+  }
+  RTS_CUDA_TRY(cudaEventRecord(sv->ev_staged[k], us));
+  sv->staged[k] = true;
+  return RTS_OK;
+}
+
+void release_update_staging(rts_server* sv) {
+  for (int k = 0; k < 2; ++k) {
+    if (sv->ev_staged[k]) {
+      if (sv->staged[k]) cudaEventSynchronize(sv->ev_staged[k]);
+      cudaEventDestroy(sv->ev_staged[k]);
+      sv->ev_staged[k] = nullptr;
+    }
+    if (sv->upd_host[k]) cudaFreeHost(sv->upd_host[k]);
+    sv->upd_host[k] = nullptr;
+    sv->upd_host_bytes[k] = 0;
+    sv->staged[k] = false;
+  }
+}
+
 // Applies the update request at the head of the queue.  Called only when no
 // launch is in flight and no part waits for a re-run, so every query
 // submitted before the update has its final pairs and every later query
 // launches after it (its stream waits on ev_update).
-int stage_and(cudaStream_t us, const void* host, size_t bytes, void** dev) {
-  if (int rc = dev_alloc(dev, bytes, us)) return rc;
-  cudaError_t e = cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, us);
-  if (e != cudaSuccess) return cuda_fail(e, "staging an update batch");
-  return RTS_OK;
-}
-
 void apply_update(rts_server* sv, Request* r) {
   cudaStream_t us = sv->update_stream;
   const double t0 = now_s();
-  int rc = RTS_OK;
-  void* d = nullptr;
-  if (!r->del.empty()) {
-    rc = stage_and(us, r->del.data(), r->del.size() * sizeof(uint64_t), &d);
-    if (!rc) rc = rts_delete(sv->ix, static_cast<const uint64_t*>(d), r->del.size(), us);
-    dev_free(d, us);
-  }
-  if (!rc && !r->upd.empty()) {
-    rc = stage_and(us, r->upd.data(), r->upd.size() * sizeof(rts_update_entry), &d);
-    if (!rc) rc = rts_update(sv->ix, static_cast<const rts_update_entry*>(d), r->upd.size(), us);
-    dev_free(d, us);
-  }
-  if (!rc && !r->ins.empty()) {
-    const uint64_t n = r->ins.size() / 4;
-    rc = stage_and(us, r->ins.data(), n * 4 * sizeof(float), &d);
-    r->first_new_id = rts_size(sv->ix);
-    if (!rc) rc = rts_insert(sv->ix, static_cast<const float*>(d), n, us);
-    dev_free(d, us);
-  }
+  void *d_del = nullptr, *d_upd = nullptr, *d_ins = nullptr;
+  int rc = stage_update(sv, r, &d_del, &d_upd, &d_ins);
+  if (!rc && d_del)
+    rc = rts_delete(sv->ix, static_cast<const uint64_t*>(d_del), r->del.size(), us);
+  if (!rc && d_upd)
+    rc = rts_update(sv->ix, static_cast<const rts_update_entry*>(d_upd), r->upd.size(), us);
+  r->first_new_id = rts_size(sv->ix);
+  if (!rc && d_ins) rc = rts_insert(sv->ix, static_cast<const float*>(d_ins), r->ins.size() / 4, us);
+  dev_free(d_del, us);
+  dev_free(d_upd, us);
+  dev_free(d_ins, us);
   r->status = rc;
   sv->update_s += now_s() - t0;
   cudaEventRecord(sv->ev_update, us);
@@ -664,11 +714,16 @@ int rts_server_create(rts_index* ix, const rts_server_config* cfg, rts_server** 
                       c.max_queries_per_launch * 24ull + c.max_parts_per_launch * 96ull;
   if (per_slot * c.slots > budget)
     return fail(RTS_ERR_OUT_OF_MEMORY, "server arenas exceed the HBM budget");
+  // The index will take update batches from the request stream: its first
+  // ones would grow its slot arrays and reserve its re-sort buffers, an
+  // allocation of the index's size inside a request's latency.  Do it now.
+  int rc = reserve_for_updates(ix, 0);
+  if (rc) return rc;
+  RTS_CUDA_TRY(cudaStreamSynchronize(0));
   auto sv = std::make_unique<rts_server>();
   sv->ix = ix;
   sv->cfg = c;
   RTS_CUDA_TRY(cudaGetDevice(&sv->device));
-  int rc = RTS_OK;
   for (uint32_t i = 0; i < c.slots && !rc; ++i) {
     sv->slots.push_back(std::make_unique<Slot>());
     rc = slot_init(sv.get(), *sv->slots.back(), c.max_queries_per_launch * 16ull,
@@ -678,10 +733,18 @@ int rts_server_create(rts_index* ix, const rts_server_config* cfg, rts_server** 
   if (!rc) {
     cudaError_t e = cudaStreamCreateWithFlags(&sv->update_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->ev_update, cudaEventDisableTiming);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+      e = cudaEventCreateWithFlags(&sv->ev_staged[k], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&sv->upd_host[k]), 8u << 20);
+      if (e == cudaSuccess) sv->upd_host_bytes[k] = 8u << 20;
+    }
     if (e != cudaSuccess) rc = cuda_fail(e, "server streams");
   }
   if (rc) {
     for (auto& sl : sv->slots) slot_free(*sl);
+    release_update_staging(sv.get());
+    if (sv->ev_update) cudaEventDestroy(sv->ev_update);
+    if (sv->update_stream) cudaStreamDestroy(sv->update_stream);
     sv->arena.destroy();
     return rc;
   }
@@ -705,6 +768,7 @@ int rts_server_destroy(rts_server* sv) {
     cudaStreamDestroy(sv->update_stream);
   }
   if (sv->ev_update) cudaEventDestroy(sv->ev_update);
+  release_update_staging(sv);
   sv->reqs.clear();
   sv->arena.destroy();
   delete sv;
