@@ -38,6 +38,7 @@ ranks.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -1201,7 +1202,12 @@ def run_other_configs(args, ctx) -> dict:
         for k, v in over.items():
             setattr(a, k, v)
         t0 = time.perf_counter()
+        # Indexes of the previous configuration are destroyed here, not during
+        # this one's timed steps (a destroy synchronises the device and returns
+        # the library's kept memory).
+        gc.collect()
         line = run_config(a, ctx)
+        gc.collect()
         ctx.torch.cuda.empty_cache()
         keep = ("value", "unit", "ms_per_step", "steps", "warmup", "config", "latency_ms",
                 "pairs_per_s", "pairs_per_step", "forms", "e2e", "roofline", "cpu_baseline",
