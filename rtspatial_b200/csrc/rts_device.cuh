@@ -74,8 +74,8 @@ __device__ __forceinline__ void ldg_box_pair(const float4* p, float4& a, float4&
 // Bulk copies into shared memory (the staged traversal scheme).  A copy is
 // issued by one thread with cp.async.bulk (the TMA unit moves the bytes from
 // L2 into shared memory without passing through L1 or registers) and
-// completes on an mbarrier whose transaction count it decrements.  No
-// multicast form is used.
+// completes on an mbarrier whose transaction count it decrements.  Each copy
+// writes the issuing CTA's own shared memory from this GPU's global memory.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
