@@ -339,6 +339,9 @@ typedef struct rts_server_stats {
   double issue_s;   /* worker thread: issuing launches (API calls, or capture + update + replay) */
 } rts_server_stats;
 int rts_server_config_default(rts_server_config* cfg);
+/* Creating a server reserves the index's update capacity (twice its used
+ * slots and ids, and the buffers of a full re-sort) so that update batches
+ * allocate nothing on the request path. */
 int rts_server_create(rts_index* index, const rts_server_config* cfg, rts_server** out);
 /* Finishes every submitted request, then stops. */
 int rts_server_destroy(rts_server* server);
