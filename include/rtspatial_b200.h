@@ -389,8 +389,7 @@ int rts_server_reset_stats(rts_server* server);
  * RTS_NOALLOC_MAX_BATCHES non-empty batches per call (RTS_ERR_CAPACITY
  * otherwise; empty batches do not count).  All calls on a device share that
  * array: calls that overlap on the GPU race.  The first call on a device looks
- * up the array's device address; make it before any stream capture.  The
- * index must already be built; inputs and outputs are the caller's, as in
+ * up the array's device address.  The index must already be built; inputs and outputs are the caller's, as in
  * rts_query_batched. */
 #define RTS_NOALLOC_MAX_BATCHES 1024
 int rts_query_batched_noalloc(rts_index* index, const rts_batch* batches, uint32_t n_batches,

@@ -1172,8 +1172,7 @@ const char* rts_version(void) { return "rtspatial_b200 0.1 (sm_100a)"; }
 // counter is cleared by each call, the descriptor area keeps the previous
 // call's contents, and calls that overlap on the GPU (other streams, other
 // threads, other indexes) race on it.  The first call on a device looks up
-// the array's device address (cudaGetSymbolAddress); make that first call
-// before any stream capture.
+// the array's device address (cudaGetSymbolAddress).
 // ---------------------------------------------------------------------------
 namespace {
 constexpr uint32_t kNoAllocMaxBatches = RTS_NOALLOC_MAX_BATCHES;
