@@ -133,6 +133,24 @@ def test_argument_validation_without_gpu():
     assert lib.rts_insert(None, None, 0, None) == L.RTS_ERR_INVALID_ARGUMENT
 
 
+def test_memory_calls_without_gpu():
+    # the library's device memory: without a GPU nothing was allocated in this
+    # process, so the stats read zero and a trim has nothing to return; bad
+    # arguments are refused
+    import torch
+    lib = L.lib()
+    r, u = ctypes.c_uint64(7), ctypes.c_uint64(7)
+    assert lib.rts_memory_pool_stats(0, ctypes.byref(r), ctypes.byref(u)) == L.RTS_OK
+    assert r.value >= u.value
+    if not torch.cuda.is_available():
+        assert r.value == 0 and u.value == 0
+        assert lib.rts_trim_memory(0) == L.RTS_OK
+    assert lib.rts_memory_pool_stats(-1, ctypes.byref(r), ctypes.byref(u)) == \
+        L.RTS_ERR_INVALID_ARGUMENT
+    assert lib.rts_memory_pool_stats(0, None, ctypes.byref(u)) == L.RTS_ERR_INVALID_ARGUMENT
+    assert lib.rts_trim_memory(64) == L.RTS_ERR_INVALID_ARGUMENT
+
+
 def test_python_mirror_surface():
     # names of rtspatial::SpatialIndex's public methods
     for m in ("Init", "Clear", "Insert", "Delete", "Update", "Query", "PrintMemoryUsage"):
